@@ -1,0 +1,160 @@
+/*
+ * amss_b200.h -- C ABI of the B200-native AMSS-NCKU evolution hot path.
+ *
+ * Two layers:
+ *
+ * 1. Drop-in entry points with the reference's Fortran symbols and argument
+ *    lists (gfortran "fortran3" mangling: lower case + trailing underscore,
+ *    every argument by reference).  A caller linked against libamss_b200.so
+ *    instead of the Fortran objects gets the same results computed on the
+ *    GPU.  Arrays are host arrays in Fortran order (i fastest), exactly as the
+ *    reference's Block::fgfs holds them; nothing is retained between calls.
+ *
+ * 2. The batched engine (amss_engine_*): blocks of every level stay resident
+ *    in HBM, one kernel launch advances all blocks of a level by one RK4
+ *    substep, and a whole step can be replayed as a CUDA graph.
+ *
+ * Return codes: 0 success; 1 NaN found in the input state (the reference's
+ * `gont`); negative values are library errors (AMSS_ERR_*), with a message
+ * available from amss_last_error().  There is no CPU fallback: without a
+ * usable CUDA device every entry point fails with AMSS_ERR_NO_DEVICE.
+ */
+#ifndef AMSS_B200_H
+#define AMSS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMSS_OK 0
+#define AMSS_NAN 1
+#define AMSS_ERR_NO_DEVICE (-1)
+#define AMSS_ERR_CUDA (-2)
+#define AMSS_ERR_ARG (-3)
+#define AMSS_ERR_UNSUPPORTED (-4)
+#define AMSS_ERR_STATE (-5)
+
+/* Last error message of the calling thread ("" if none). */
+const char* amss_last_error(void);
+/* Library version string. */
+const char* amss_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Drop-in per-block kernels
+ * ------------------------------------------------------------------------- */
+
+/* Replaces compute_rhs_bssn (bssn_rhs.f90:5-1184; C prototype bssn_rhs.h:37-54,
+ * called per block from bssn_class.C:3059 and :3430).  GAUGE 0, Cell,
+ * ghost_width 3.  Outputs: 24 RHS, 18 physical Christoffel symbols, 6 Ricci
+ * components, and (co == 0) the 7 constraint residuals.  Returns 1 without
+ * touching any output when the input state holds a NaN (bssn_rhs.f90:110-138). */
+int compute_rhs_bssn_(
+    int* ex, double* T, double* X, double* Y, double* Z,
+    double* chi, double* trK, double* dxx, double* gxy, double* gxz, double* dyy, double* gyz, double* dzz,
+    double* Axx, double* Axy, double* Axz, double* Ayy, double* Ayz, double* Azz,
+    double* Gamx, double* Gamy, double* Gamz,
+    double* Lap, double* betax, double* betay, double* betaz,
+    double* dtSfx, double* dtSfy, double* dtSfz,
+    double* chi_rhs, double* trK_rhs,
+    double* gxx_rhs, double* gxy_rhs, double* gxz_rhs, double* gyy_rhs, double* gyz_rhs, double* gzz_rhs,
+    double* Axx_rhs, double* Axy_rhs, double* Axz_rhs, double* Ayy_rhs, double* Ayz_rhs, double* Azz_rhs,
+    double* Gamx_rhs, double* Gamy_rhs, double* Gamz_rhs,
+    double* Lap_rhs, double* betax_rhs, double* betay_rhs, double* betaz_rhs,
+    double* dtSfx_rhs, double* dtSfy_rhs, double* dtSfz_rhs,
+    double* rho, double* Sx, double* Sy, double* Sz,
+    double* Sxx, double* Sxy, double* Sxz, double* Syy, double* Syz, double* Szz,
+    double* Gamxxx, double* Gamxxy, double* Gamxxz, double* Gamxyy, double* Gamxyz, double* Gamxzz,
+    double* Gamyxx, double* Gamyxy, double* Gamyxz, double* Gamyyy, double* Gamyyz, double* Gamyzz,
+    double* Gamzxx, double* Gamzxy, double* Gamzxz, double* Gamzyy, double* Gamzyz, double* Gamzzz,
+    double* Rxx, double* Rxy, double* Rxz, double* Ryy, double* Ryz, double* Rzz,
+    double* ham_Res, double* movx_Res, double* movy_Res, double* movz_Res,
+    double* Gmx_Res, double* Gmy_Res, double* Gmz_Res,
+    int* Symmetry, int* Lev, double* eps, int* co);
+
+/* Replaces rungekutta4_rout (rungekutta4_rout.f90:94-139; rungekutta4_rout.h:34-38,
+ * called per field from bssn_class.C:3119 and :3430-3525).  RK4 = 0..3. */
+int rungekutta4_rout_(int* ex, double* dT, double* f0, double* f1, double* f_rhs, int* RK4);
+
+/* Replaces sommerfeld_routbam (sommerfeld_rout.f90:223-449; sommerfeld_rout.h:33-37,
+ * called per field on level 0 from bssn_class.C:3109). */
+void sommerfeld_routbam_(int* ex, double* X, double* Y, double* Z,
+                         double* xmin, double* ymin, double* zmin, double* xmax, double* ymax, double* zmax,
+                         double* f_rhs, double* f0, double* velocity, double* SoA, int* Symmetry);
+
+/* Replaces sommerfeld_rout (sommerfeld_rout.f90:9-221; sommerfeld_rout.h:26-30,
+ * called per field on levels > 0 from bssn_class.C:3127).  Only precor == 1,
+ * the branch on the evolution path (copy f0 onto the patch faces), is
+ * implemented; other values fail with AMSS_ERR_UNSUPPORTED. */
+void sommerfeld_rout_(int* ex, double* X, double* Y, double* Z,
+                      double* xmin, double* ymin, double* zmin, double* xmax, double* ymax, double* zmax,
+                      double* dT, double* chi0, double* Lap0, double* f0, double* f, double* SoA,
+                      int* Symmetry, int* precor);
+
+/* Replaces enforce_ga (enforce_algebra.f90:72-133; enforce_algebra.h:26-28,
+ * called from bssn_class.C:3052 and :3416). In place. */
+void enforce_ga_(int* ex, double* dxx, double* gxy, double* gxz, double* dyy, double* gyz, double* dzz,
+                 double* Axx, double* Axy, double* Axz, double* Ayy, double* Ayz, double* Azz);
+
+/* Replaces lowerboundset (fmisc.f90:1644-1657; fmisc.h:210, called from
+ * bssn_class.C:3156 and :3525). In place. */
+void lowerboundset_(int* ex, double* chi, double* tinny);
+
+/* ---------------------------------------------------------------------------
+ * Batched engine: device-resident blocks, one launch per level substep.
+ * ------------------------------------------------------------------------- */
+
+typedef struct amss_engine amss_engine;
+
+typedef struct {
+  int precision;      /* 0: FP64; 1: mixed (FP32 stencils/stages, FP64 state and accumulator) */
+  int symmetry;       /* 0 none, 1 equatorial, 2 octant (ABE::Symmetry) */
+  double eps;         /* KO dissipation (ABE::... dissipation) */
+  double chitiny;     /* chi floor as the reference stores it: BSSN::chitiny - 1 */
+} amss_params;
+
+/* Create an engine on the current CUDA device.  Returns NULL on failure. */
+amss_engine* amss_engine_create(const amss_params* prm);
+void amss_engine_destroy(amss_engine* e);
+
+/* Add one block of `level`: ex points per direction, its cell-centred bbox
+ * (Block::bbox, coordinates X[j] = bbox_lo + (j + 0.5) h) and the bbox of the
+ * patch it belongs to (decides which faces take the outer boundary rule).
+ * Returns the block id (>= 0) or an error code. */
+int amss_engine_add_block(amss_engine* e, int level, const int ex[3], const double bbox[6],
+                          const double patch_bbox[6]);
+
+/* Allocate HBM for all blocks and build the per-level work lists. */
+int amss_engine_commit(amss_engine* e);
+
+/* Copy one block's 24-field state (host, Fortran order, field-major) in/out. */
+int amss_engine_set_state(amss_engine* e, int block, const double* host_state);
+int amss_engine_get_state(amss_engine* e, int block, double* host_state);
+/* Device pointer of field 0 of a block's state and the field stride in elements. */
+int amss_engine_state_device(amss_engine* e, int block, double** dptr, long long* field_stride);
+
+/* Apply enforce_ga to every block's state once (the reference does this at
+ * the start of every step; the engine then keeps states in that form). */
+int amss_engine_enforce(amss_engine* e);
+
+/* Advance every block of `level` by one RK4 step of size dt on the engine's
+ * stream (asynchronous).  Single-level hierarchies only in this form. */
+int amss_engine_step_level(amss_engine* e, int level, double dt);
+
+/* Capture `nsteps` calls of amss_engine_step_level(level, dt) as one CUDA
+ * graph and replay it `replays` times. */
+int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int replays);
+
+/* Wait for the engine's stream; returns 1 if any substep saw a NaN, else 0. */
+int amss_engine_sync(amss_engine* e);
+
+/* The engine's CUDA stream (cudaStream_t), for timing with events. */
+void* amss_engine_stream(amss_engine* e);
+
+/* Number of kernel launches the engine issued so far. */
+long long amss_engine_launch_count(amss_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMSS_B200_H */

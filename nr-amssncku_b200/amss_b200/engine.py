@@ -1,0 +1,94 @@
+"""Batched, device-resident evolution engine (amss_engine_* of include/amss_b200.h).
+
+The engine plays the role of the reference's level step (bssn_class::Step,
+bssn_class.C:2981-3915): it owns every block's state in HBM and advances all
+blocks of a level by one RK4 step with four kernel launches.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import _DP, AmssError, check, last_error, lib
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("symmetry", ctypes.c_int),
+                ("eps", ctypes.c_double), ("chitiny", ctypes.c_double)]
+
+
+class Engine:
+    """One hierarchy of blocks on the current CUDA device.
+
+    precision: "fp64" or "mixed" (FP32 stencils and stages, FP64 state,
+    accumulator and update).  chitiny is BSSN::chitiny as the par file gives
+    it (1e-5); the engine shifts it by -1 as bssn_class.C:179 does."""
+
+    def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5):
+        prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0)
+        self._h = lib().amss_engine_create(ctypes.byref(prm))
+        if not self._h:
+            raise AmssError("amss_engine_create failed: " + last_error())
+        self.blocks = []
+
+    def close(self):
+        if self._h:
+            lib().amss_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_block(self, level, ex, bbox, patch_bbox):
+        exa = (ctypes.c_int * 3)(*ex)
+        bb = (ctypes.c_double * 6)(*bbox)
+        pb = (ctypes.c_double * 6)(*patch_bbox)
+        bid = check(lib().amss_engine_add_block(self._h, level, exa, bb, pb), "amss_engine_add_block")
+        self.blocks.append(tuple(ex))
+        return bid
+
+    def commit(self):
+        check(lib().amss_engine_commit(self._h), "amss_engine_commit")
+
+    def set_state(self, block, state):
+        state = np.ascontiguousarray(state, dtype=np.float64)
+        check(lib().amss_engine_set_state(self._h, block, state.ctypes.data_as(_DP)), "amss_engine_set_state")
+
+    def get_state(self, block, out=None):
+        ex = self.blocks[block]
+        if out is None:
+            out = np.empty((24, ex[2], ex[1], ex[0]))
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (24, ex[2], ex[1], ex[0]):
+            raise AmssError("get_state: out must be a C-contiguous float64 (24, ez, ey, ex) array")
+        check(lib().amss_engine_get_state(self._h, block, out.ctypes.data_as(_DP)), "amss_engine_get_state")
+        return out
+
+    def state_device(self, block):
+        ptr = ctypes.c_void_p()
+        fs = ctypes.c_longlong()
+        check(lib().amss_engine_state_device(self._h, block, ctypes.byref(ptr), ctypes.byref(fs)),
+              "amss_engine_state_device")
+        return ptr.value, fs.value
+
+    def enforce(self):
+        check(lib().amss_engine_enforce(self._h), "amss_engine_enforce")
+
+    def step(self, level, dt):
+        check(lib().amss_engine_step_level(self._h, level, dt), "amss_engine_step_level")
+
+    def run_graph(self, level, dt, nsteps, replays=1):
+        check(lib().amss_engine_run_graph(self._h, level, dt, nsteps, replays), "amss_engine_run_graph")
+
+    def sync(self):
+        """Waits for the engine's stream; returns 1 if a NaN was seen."""
+        return check(lib().amss_engine_sync(self._h), "amss_engine_sync")
+
+    @property
+    def stream(self):
+        return lib().amss_engine_stream(self._h)
+
+    @property
+    def launches(self):
+        return lib().amss_engine_launch_count(self._h)

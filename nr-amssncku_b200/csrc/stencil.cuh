@@ -1,0 +1,199 @@
+// stencil.cuh -- point access and finite-difference stencils of the BSSN kernels.
+//
+// One thread owns one grid point (i, j, k) of one block.  Stencil values are
+// read straight from HBM/L2 through the read-only path; the stencil formulas
+// and their association order are those of diff_new.f90:946-1528
+// (fderivs/fdderivs, "for bam comparison" branch), lopsidediff.f90:321-481
+// and kodiss.f90:190-207, so that FP64 results agree with the reference to
+// round-off.
+#pragma once
+#include "amss_common.cuh"
+
+namespace amss {
+
+// Per-block stencil coefficients, computed on the host in double exactly as
+// the Fortran computes them (e.g. d12dx = ONE/F12/dX) and then cast to T.
+template <typename T>
+struct Coef {
+  T d12[3];          // 1/12/dx
+  T d2[3];           // 1/2/dx
+  T Fdd[3];          // (1/12)/(dx*dx)
+  T Sdd[3];          // 1/(dx*dx)
+  T Fxy, Fxz, Fyz;   // (1/144)/(dx*dy)
+  T Sxy, Sxz, Syz;   // 0.25/(dx*dy)
+  T h[3];            // dx itself (KO divides by it)
+  T ko;              // eps/64
+};
+
+// Point accessor.  With SYMM == false, offsets are applied directly: callers
+// only step outside [0, ex) where the reference reads its symmetry pad.  With
+// SYMM == true every access mirrors negative indices cell-centred,
+// f(-m) = f(m-1) * parity (fmisc.f90:877-901), which also covers that pad.
+template <typename SI, bool SYMM>
+struct Pt {
+  const SI* __restrict__ base;  // field 0 of the block
+  long long fs;                 // field stride
+  long long p;                  // linear index of the point
+  long long sy, sz;             // strides of j and k
+  int i, j, k;                  // 0-based indices
+  int ex0, ex1, ex2;
+
+  template <typename T, int F>
+  __device__ __forceinline__ T v(int di, int dj, int dk) const {
+    if constexpr (!SYMM) {
+      return (T)__ldg(base + F * fs + p + di + dj * sy + dk * sz);
+    } else {
+      int ii = i + di, jj = j + dj, kk = k + dk;
+      bool neg = false;
+      if (ii < 0) { ii = -ii - 1; neg ^= (soa_sign(F, 0) < 0); }
+      if (jj < 0) { jj = -jj - 1; neg ^= (soa_sign(F, 1) < 0); }
+      if (kk < 0) { kk = -kk - 1; neg ^= (soa_sign(F, 2) < 0); }
+      T x = (T)__ldg(base + F * fs + ii + jj * sy + kk * sz);
+      return neg ? -x : x;
+    }
+  }
+  // value with the pad rule even when SYMM == false (lopsided reads index -1)
+  template <typename T, int F>
+  __device__ __forceinline__ T vpad(int di, int dj, int dk) const {
+    int ii = i + di, jj = j + dj, kk = k + dk;
+    bool neg = false;
+    if (ii < 0) { ii = -ii - 1; neg ^= (soa_sign(F, 0) < 0); }
+    if (jj < 0) { jj = -jj - 1; neg ^= (soa_sign(F, 1) < 0); }
+    if (kk < 0) { kk = -kk - 1; neg ^= (soa_sign(F, 2) < 0); }
+    T x = (T)__ldg(base + F * fs + ii + jj * sy + kk * sz);
+    return neg ? -x : x;
+  }
+};
+
+template <int D>
+__device__ __forceinline__ constexpr int ax(int d) { return D == d ? 1 : 0; }
+
+// ---- first derivatives (fderivs), one direction D ---------------------------
+// 4th order: d12 * (f(-2) - 8 f(-1) + 8 f(+1) - f(+2))
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T d1o4(const P& q, const Coef<T>& C) {
+  const T EIT = T(8);
+  return C.d12[D] * (q.template v<T, F>(-2 * ax<D>(0), -2 * ax<D>(1), -2 * ax<D>(2)) -
+                     EIT * q.template v<T, F>(-ax<D>(0), -ax<D>(1), -ax<D>(2)) +
+                     EIT * q.template v<T, F>(ax<D>(0), ax<D>(1), ax<D>(2)) -
+                     q.template v<T, F>(2 * ax<D>(0), 2 * ax<D>(1), 2 * ax<D>(2)));
+}
+// 2nd order: d2 * (-f(-1) + f(+1))
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T d1o2(const P& q, const Coef<T>& C) {
+  return C.d2[D] * (-q.template v<T, F>(-ax<D>(0), -ax<D>(1), -ax<D>(2)) +
+                    q.template v<T, F>(ax<D>(0), ax<D>(1), ax<D>(2)));
+}
+
+// Gradient of field F with the reference's joint order gate: ord 2 = 4th order,
+// 1 = 2nd order, 0 = derivative is zero (diff_new.f90:1084-1096).
+template <typename T, int F, typename P>
+__device__ __forceinline__ void grad(const P& q, const Coef<T>& C, int ord, T& fx, T& fy, T& fz) {
+  if (ord == 2) {
+    fx = d1o4<T, F, 0>(q, C); fy = d1o4<T, F, 1>(q, C); fz = d1o4<T, F, 2>(q, C);
+  } else if (ord == 1) {
+    fx = d1o2<T, F, 0>(q, C); fy = d1o2<T, F, 1>(q, C); fz = d1o2<T, F, 2>(q, C);
+  } else {
+    fx = T(0); fy = T(0); fz = T(0);
+  }
+}
+
+// ---- second derivatives (fdderivs) ------------------------------------------
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T d2o4(const P& q, const Coef<T>& C) {
+  const T F16 = T(16), F30 = T(30);
+  return C.Fdd[D] * (-q.template v<T, F>(-2 * ax<D>(0), -2 * ax<D>(1), -2 * ax<D>(2)) +
+                     F16 * q.template v<T, F>(-ax<D>(0), -ax<D>(1), -ax<D>(2)) -
+                     F30 * q.template v<T, F>(0, 0, 0) -
+                     q.template v<T, F>(2 * ax<D>(0), 2 * ax<D>(1), 2 * ax<D>(2)) +
+                     F16 * q.template v<T, F>(ax<D>(0), ax<D>(1), ax<D>(2)));
+}
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T d2o2(const P& q, const Coef<T>& C) {
+  const T TWO = T(2);
+  return C.Sdd[D] * (q.template v<T, F>(-ax<D>(0), -ax<D>(1), -ax<D>(2)) - TWO * q.template v<T, F>(0, 0, 0) +
+                     q.template v<T, F>(ax<D>(0), ax<D>(1), ax<D>(2)));
+}
+// mixed derivative in directions (A, B), A < B: 4th order 16-point cross
+// stencil / 144 dA dB, rows taken along A and combined along B.
+template <typename T, int F, int A, int B, typename P>
+__device__ __forceinline__ T row4(const P& q, int ob) {
+  const T F8 = T(8);
+  return q.template v<T, F>(-2 * ax<A>(0) + ob * ax<B>(0), -2 * ax<A>(1) + ob * ax<B>(1), -2 * ax<A>(2) + ob * ax<B>(2)) -
+         F8 * q.template v<T, F>(-ax<A>(0) + ob * ax<B>(0), -ax<A>(1) + ob * ax<B>(1), -ax<A>(2) + ob * ax<B>(2)) +
+         F8 * q.template v<T, F>(ax<A>(0) + ob * ax<B>(0), ax<A>(1) + ob * ax<B>(1), ax<A>(2) + ob * ax<B>(2)) -
+         q.template v<T, F>(2 * ax<A>(0) + ob * ax<B>(0), 2 * ax<A>(1) + ob * ax<B>(1), 2 * ax<A>(2) + ob * ax<B>(2));
+}
+template <typename T, int F, int A, int B, typename P>
+__device__ __forceinline__ T dmo4(const P& q, T coef) {
+  const T F8 = T(8);
+  return coef * (row4<T, F, A, B>(q, -2) - F8 * row4<T, F, A, B>(q, -1) + F8 * row4<T, F, A, B>(q, 1) -
+                 row4<T, F, A, B>(q, 2));
+}
+template <typename T, int F, int A, int B, typename P>
+__device__ __forceinline__ T dmo2(const P& q, T coef) {
+  return coef * (q.template v<T, F>(-ax<A>(0) - ax<B>(0), -ax<A>(1) - ax<B>(1), -ax<A>(2) - ax<B>(2)) -
+                 q.template v<T, F>(ax<A>(0) - ax<B>(0), ax<A>(1) - ax<B>(1), ax<A>(2) - ax<B>(2)) -
+                 q.template v<T, F>(-ax<A>(0) + ax<B>(0), -ax<A>(1) + ax<B>(1), -ax<A>(2) + ax<B>(2)) +
+                 q.template v<T, F>(ax<A>(0) + ax<B>(0), ax<A>(1) + ax<B>(1), ax<A>(2) + ax<B>(2)));
+}
+
+// Hessian of F: fxx fxy fxz fyy fyz fzz (fdderivs output order).
+template <typename T, int F, typename P>
+__device__ __forceinline__ void hess(const P& q, const Coef<T>& C, int ord, T& fxx, T& fxy, T& fxz, T& fyy,
+                                     T& fyz, T& fzz) {
+  if (ord == 2) {
+    fxx = d2o4<T, F, 0>(q, C); fyy = d2o4<T, F, 1>(q, C); fzz = d2o4<T, F, 2>(q, C);
+    fxy = dmo4<T, F, 0, 1>(q, C.Fxy); fxz = dmo4<T, F, 0, 2>(q, C.Fxz); fyz = dmo4<T, F, 1, 2>(q, C.Fyz);
+  } else if (ord == 1) {
+    fxx = d2o2<T, F, 0>(q, C); fyy = d2o2<T, F, 1>(q, C); fzz = d2o2<T, F, 2>(q, C);
+    fxy = dmo2<T, F, 0, 1>(q, C.Sxy); fxz = dmo2<T, F, 0, 2>(q, C.Sxz); fyz = dmo2<T, F, 1, 2>(q, C.Syz);
+  } else {
+    fxx = fxy = fxz = fyy = fyz = fzz = T(0);
+  }
+}
+
+// ---- upwinded advection (lopsided), one direction ---------------------------
+// Returns r + beta * D^upwind f along D following lopsidediff.f90:321-481;
+// `add1` is 1 when the advected array is the full metric g = d + 1.
+// lo/hi are the reference's imin/imax in 0-based form.
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T lop_dir(const P& q, const Coef<T>& C, T r, T b, int idx, int lo, int hi, T add1) {
+  const T F3 = T(3), F10 = T(10), F18 = T(18), F6 = T(6), EIT = T(8);
+  auto f = [&](int o) -> T {
+    return q.template vpad<T, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)) + add1;
+  };
+  const T bd = b * C.d12[D];
+  if (b > T(0)) {
+    if (idx + 3 <= hi)
+      r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+    else if (idx + 2 <= hi)
+      r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+    else if (idx + 1 <= hi)
+      r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+  } else if (b < T(0)) {
+    if (idx - 3 >= lo)
+      r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+    else if (idx - 2 >= lo)
+      r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+    else if (idx - 1 >= lo)
+      r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+  }
+  return r;
+}
+
+// ---- Kreiss-Oliger, combined directions (kodiss.f90:190-207) ----------------
+template <typename T, int F, int D, typename P>
+__device__ __forceinline__ T ko_line(const P& q) {
+  const T SIX = T(6), FIT = T(15), TWT = T(20);
+  auto f = [&](int o) -> T { return q.template v<T, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)); };
+  return (f(-3) + f(3)) - SIX * (f(-2) + f(2)) + FIT * (f(-1) + f(1)) - TWT * f(0);
+}
+
+template <typename T>
+__device__ __forceinline__ T divh(T a, T h) {
+  if constexpr (sizeof(T) == 8) return a / h;   // the reference divides
+  else return a * (T(1) / h);
+}
+
+}  // namespace amss
