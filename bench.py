@@ -30,7 +30,10 @@ sys.path.insert(0, os.path.join(ROOT, "nr-amssncku_b200"))
 
 METRIC = "BSSN RK4 zone-updates/s on 1 B200: FP64 vs mixed, %HBM peak; adjoint/fwd ratio"
 NF = 24
-BYTES_PER_ZONE = {"fp64": 17 * NF * 8, "mixed": 112 * NF}   # algorithmic HBM bytes per zone-update
+# algorithmic HBM bytes per zone-update: every field array read or written once per
+# substep, 17 words per field per step.  Mixed: FP32 stages for 22 fields, FP64
+# stages for chi and alpha, FP64 U0/K/U_new: 22 * 112 + 2 * 136.
+BYTES_PER_ZONE = {"fp64": 17 * NF * 8, "mixed": 22 * 112 + 2 * 136}
 
 
 def workload(name):
@@ -133,7 +136,6 @@ def run_ours(args, rank, world):
     b = eng.add_block(0, (n, n, n), bbox, bbox)
     eng.commit()
     eng.set_state(b, st0)
-    eng.enforce()
     stream = torch.cuda.ExternalStream(eng.stream)
 
     # warm-up, then K timed steps bracketed by a barrier + synchronize

@@ -110,6 +110,7 @@ typedef struct {
   int symmetry;       /* 0 none, 1 equatorial, 2 octant (ABE::Symmetry) */
   double eps;         /* KO dissipation (ABE::... dissipation) */
   double chitiny;     /* chi floor as the reference stores it: BSSN::chitiny - 1 */
+  int kernel;         /* 0: split substep (stencil pass + pointwise pass, default); 1: fused single pass */
 } amss_params;
 
 /* Create an engine on the current CUDA device.  Returns NULL on failure. */
@@ -131,6 +132,36 @@ int amss_engine_set_state(amss_engine* e, int block, const double* host_state);
 int amss_engine_get_state(amss_engine* e, int block, double* host_state);
 /* Device pointer of field 0 of a block's state and the field stride in elements. */
 int amss_engine_state_device(amss_engine* e, int block, double** dptr, long long* field_stride);
+
+/* AMR hierarchies: the grid origin (coordinate of the lower face of global
+ * cell 0 on every level) and the level-0 cell size; level l has cell size
+ * h0 / 2^l and coarse cell k has the fine children 2k, 2k+1. */
+int amss_engine_set_grid(amss_engine* e, const double x0[3], double h0);
+
+/* Add one block of an AMR level.  org: global level index of array element 0;
+ * ex: array extent; [own_lo, own_hi): the cells the block owns (the rest of its
+ * array are ghost cells, ghost_width 3, filled from their owners after every
+ * substep as Parallel::Sync does); [phys_lo, phys_hi): the physical box of the
+ * block's patch, which on levels > 0 is surrounded by `buffer` cells
+ * (buffer_width 6) filled by prolongation from the parent level after each step
+ * (Parallel::OutBdLow2Hi).  `patch` identifies the patch within its level.
+ * Returns the block id or an error code. */
+int amss_engine_add_amr_block(amss_engine* e, int level, int patch, const int org[3], const int ex[3],
+                              const int own_lo[3], const int own_hi[3], const int phys_lo[3],
+                              const int phys_hi[3], int buffer);
+
+/* One Berger-Oliger coarse step of the whole hierarchy (bssn_class::RecursiveStep,
+ * bssn_class.C:2323-2414, with RPS 1 and time refinement from level 1): level l
+ * takes 2^l RK4 steps of dt0 / 2^l, each followed by restriction into and
+ * prolongation from its parent (bssn_class::RestrictProlong, :5724-5903) with
+ * quadratic time interpolation of the parent at intermediate times. */
+int amss_engine_coarse_step(amss_engine* e, double dt0);
+
+/* Capture `nsteps` coarse steps as one CUDA graph and replay it `replays` times. */
+int amss_engine_run_coarse_graph(amss_engine* e, double dt0, int nsteps, int replays);
+
+/* Points (array cells of all blocks) of a level. */
+long long amss_engine_level_points(amss_engine* e, int level);
 
 /* Apply enforce_ga to every block's state once (the reference does this at
  * the start of every step; the engine then keeps states in that form). */

@@ -48,6 +48,12 @@ def lib():
     L.amss_engine_sync.argtypes = [ctypes.c_void_p]
     L.amss_engine_stream.argtypes = [ctypes.c_void_p]
     L.amss_engine_stream.restype = ctypes.c_void_p
+    L.amss_engine_set_grid.argtypes = [ctypes.c_void_p, _DP, ctypes.c_double]
+    L.amss_engine_add_amr_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [_IP] * 6 + [ctypes.c_int]
+    L.amss_engine_coarse_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    L.amss_engine_run_coarse_graph.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_level_points.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.amss_engine_level_points.restype = ctypes.c_longlong
     L.amss_engine_launch_count.argtypes = [ctypes.c_void_p]
     L.amss_engine_launch_count.restype = ctypes.c_longlong
     _lib = L

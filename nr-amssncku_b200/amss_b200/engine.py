@@ -13,18 +13,20 @@ from ._lib import _DP, AmssError, check, last_error, lib
 
 class _Params(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("symmetry", ctypes.c_int),
-                ("eps", ctypes.c_double), ("chitiny", ctypes.c_double)]
+                ("eps", ctypes.c_double), ("chitiny", ctypes.c_double), ("kernel", ctypes.c_int)]
 
 
 class Engine:
     """One hierarchy of blocks on the current CUDA device.
 
     precision: "fp64" or "mixed" (FP32 stencils and stages, FP64 state,
-    accumulator and update).  chitiny is BSSN::chitiny as the par file gives
+    accumulator and update).  kernel: "split" (a stencil pass through shared
+    memory, then the pointwise RHS and RK4 update) or "fused" (one pass,
+    every stencil from global memory).  chitiny is BSSN::chitiny as the par file gives
     it (1e-5); the engine shifts it by -1 as bssn_class.C:179 does."""
 
-    def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5):
-        prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0)
+    def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5, kernel="split"):
+        prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0, 0 if kernel == "split" else 1)
         self._h = lib().amss_engine_create(ctypes.byref(prm))
         if not self._h:
             raise AmssError("amss_engine_create failed: " + last_error())
@@ -48,6 +50,40 @@ class Engine:
         bid = check(lib().amss_engine_add_block(self._h, level, exa, bb, pb), "amss_engine_add_block")
         self.blocks.append(tuple(ex))
         return bid
+
+    def set_grid(self, x0, h0):
+        check(lib().amss_engine_set_grid(self._h, (ctypes.c_double * 3)(*x0), h0), "amss_engine_set_grid")
+
+    def add_amr_block(self, level, patch, org, ex, own_lo, own_hi, phys_lo, phys_hi, buffer):
+        I3 = ctypes.c_int * 3
+        bid = check(lib().amss_engine_add_amr_block(self._h, level, patch, I3(*org), I3(*ex), I3(*own_lo), I3(*own_hi),
+                                                    I3(*phys_lo), I3(*phys_hi), buffer), "amss_engine_add_amr_block")
+        self.blocks.append(tuple(ex))
+        return bid
+
+    @classmethod
+    def from_hierarchy(cls, H, **kw):
+        """An engine holding every block of an amss_b200.hierarchy.Hierarchy,
+        block ids equal to their index in H.blocks."""
+        e = cls(**kw)
+        e.set_grid((H.x0,) * 3, H.h0)
+        for lev, patches in enumerate(H.levels):
+            for pid, p in enumerate(patches):
+                for bi in p.blocks:
+                    b = H.blocks[bi]
+                    got = e.add_amr_block(lev, pid, b.org, b.ex, b.own_lo, b.own_hi, p.lo, p.hi, p.buffer)
+                    assert got == bi
+        e.commit()
+        return e
+
+    def coarse_step(self, dt0):
+        check(lib().amss_engine_coarse_step(self._h, dt0), "amss_engine_coarse_step")
+
+    def run_coarse_graph(self, dt0, nsteps, replays=1):
+        check(lib().amss_engine_run_coarse_graph(self._h, dt0, nsteps, replays), "amss_engine_run_coarse_graph")
+
+    def level_points(self, level):
+        return lib().amss_engine_level_points(self._h, level)
 
     def commit(self):
         check(lib().amss_engine_commit(self._h), "amss_engine_commit")

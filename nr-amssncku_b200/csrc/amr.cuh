@@ -1,0 +1,225 @@
+// amr.cuh -- device side of the AMR data movement (ghost sync, restriction,
+// prolongation, time interpolation) between blocks resident in HBM.
+//
+// Every operation is a list of boxes in global level indices; a box names a
+// destination block and a source block.  Threads are mapped to box points
+// through a tile list (128 points per tile), so one launch serves all boxes
+// of a level, whatever their sizes.  Each thread moves all 24 fields of one
+// point.  Nothing here applies enforce_ga: as in the reference, restricted and
+// prolonged values are enforced by the pass at the start of the next step.
+#pragma once
+#include "amr_types.cuh"
+
+namespace amss {
+
+__device__ __forceinline__ long long amr_idx(const AmrBlock& b, int gi, int gj, int gk) {
+  return (long long)(gi - b.org[0]) + (long long)b.ex[0] * ((long long)(gj - b.org[1]) + (long long)b.ex[1] * (gk - b.org[2]));
+}
+__device__ __forceinline__ bool amr_inside(const AmrBlock& b, int gi, int gj, int gk) {
+  return gi >= b.org[0] && gi < b.org[0] + b.ex[0] && gj >= b.org[1] && gj < b.org[1] + b.ex[1] &&
+         gk >= b.org[2] && gk < b.org[2] + b.ex[2];
+}
+__device__ __forceinline__ double* amr_state(const AmrBlock& b) { return b.tl[b.lvl[0]]; }
+
+// Same-level ghost fill: copy the 24 fields of each box point from src to dst.
+template <typename SS>
+__global__ void k_amr_sync(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
+                           const int2* __restrict__ tiles, int ntiles, int which, unsigned* status) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBox& bx = boxes[tile.x];
+    const int p = tile.y + threadIdx.x;
+    const int np = bx.n[0] * bx.n[1] * bx.n[2];
+    if (p >= np) continue;
+    const int gi = bx.lo[0] + p % bx.n[0], gj = bx.lo[1] + (p / bx.n[0]) % bx.n[1], gk = bx.lo[2] + p / (bx.n[0] * bx.n[1]);
+    const AmrBlock& D = blocks[bx.dst];
+    const AmrBlock& S = blocks[bx.src];
+    if (!amr_inside(D, gi, gj, gk) || !amr_inside(S, gi, gj, gk)) { atomicOr(status, ST_BAD_ARG); continue; }
+    const long long od = amr_idx(D, gi, gj, gk), os = amr_idx(S, gi, gj, gk);
+    if (which == BUF_STATE || which == BUF_TEMP) {
+      const double* s = which == BUF_STATE ? amr_state(S) : S.K;
+      double* d = which == BUF_STATE ? amr_state(D) : D.K;
+      for (int f = 0; f < 24; ++f) d[f * D.fs + od] = s[f * S.fs + os];
+    } else {
+      const int sl = which == BUF_STAGE_A ? 0 : 1;
+      const SS* s = (const SS*)S.st[sl];
+      SS* d = (SS*)D.st[sl];
+      for (int f = 0; f < 24; ++f) d[f * D.fs + od] = s[f * S.fs + os];
+      if constexpr (sizeof(SS) == 4) {
+        D.side[sl][od] = S.side[sl][os];
+        D.side[sl][D.fs + od] = S.side[sl][S.fs + os];
+      }
+    }
+  }
+}
+
+// prolongrestrict_cell.f90:1937-1942 and :2350
+__device__ __constant__ double kProlongW[6] = {7.7e1 / 8.192e3, -6.93e2 / 8.192e3, 3.465e3 / 4.096e3,
+                                               1.155e3 / 4.096e3, -4.95e2 / 8.192e3, 6.3e1 / 8.192e3};
+
+// Fine buffer cells of dst (fine) from the parent level's src block:
+// prolong3 (prolongrestrict_cell.f90:1915-2164), z then y then x; g odd is
+// the right child of k = g >> 1 (coarse k-2..k+3, weights C1..C6), g even
+// the left child (coarse k-3..k+2, weights C6..C1).
+__global__ void k_amr_prolong(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
+                              const int2* __restrict__ tiles, int ntiles, int from_temp, int enforce,
+                              unsigned* status) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBox& bx = boxes[tile.x];
+    const int p = tile.y + threadIdx.x;
+    const int np = bx.n[0] * bx.n[1] * bx.n[2];
+    if (p >= np) continue;
+    const int g[3] = {bx.lo[0] + p % bx.n[0], bx.lo[1] + (p / bx.n[0]) % bx.n[1], bx.lo[2] + p / (bx.n[0] * bx.n[1])};
+    const AmrBlock& D = blocks[bx.dst];
+    const AmrBlock& S = blocks[bx.src];
+    int s0[3];
+    bool rev[3];
+    for (int d = 0; d < 3; ++d) {
+      const int k = g[d] >> 1;
+      rev[d] = (g[d] & 1) == 0;
+      s0[d] = rev[d] ? k - 3 : k - 2;
+    }
+    if (!amr_inside(D, g[0], g[1], g[2]) || !amr_inside(S, s0[0], s0[1], s0[2]) ||
+        !amr_inside(S, s0[0] + 5, s0[1] + 5, s0[2] + 5)) {
+      atomicOr(status, ST_BAD_ARG);
+      continue;
+    }
+    const double* src = from_temp ? S.K : amr_state(S);
+    const long long sy = S.ex[0], sz = (long long)S.ex[0] * S.ex[1];
+    const long long base = amr_idx(S, s0[0], s0[1], s0[2]);
+    double w[3][6];
+    for (int d = 0; d < 3; ++d)
+      for (int m = 0; m < 6; ++m) w[d][m] = kProlongW[rev[d] ? 5 - m : m];
+    double out[24];
+    for (int f = 0; f < 24; ++f) {
+      const double* q = src + f * S.fs + base;
+      double tmp1[6];
+      for (int a = 0; a < 6; ++a) {
+        double t1 = 0.0;
+        for (int b = 0; b < 6; ++b) {
+          const double* r = q + a + b * sy;
+          double t2 = __dmul_rn(w[2][0], r[0]);
+          for (int m = 1; m < 6; ++m) t2 = __dadd_rn(t2, __dmul_rn(w[2][m], r[m * sz]));
+          t1 = b == 0 ? __dmul_rn(w[1][0], t2) : __dadd_rn(t1, __dmul_rn(w[1][b], t2));
+        }
+        tmp1[a] = t1;
+      }
+      double v = __dmul_rn(w[0][0], tmp1[0]);
+      for (int a = 1; a < 6; ++a) v = __dadd_rn(v, __dmul_rn(w[0][a], tmp1[a]));
+      out[f] = v;
+    }
+    if (enforce) enforce_ga_point(out + F_GXX, out + F_AXX);  // off on the evolution path
+    double* dst = amr_state(D);
+    const long long od = amr_idx(D, g[0], g[1], g[2]);
+    for (int f = 0; f < 24; ++f) dst[f * D.fs + od] = out[f];
+  }
+}
+
+// Coarse cells of dst (coarse) from fine src: restrict3
+// (prolongrestrict_cell.f90:2330-2468): fine 2k-2..2k+3 with weights
+// C1 C2 C3 C3 C2 C1, z then y then x.  Writes the current state or the
+// time-interpolated temp.
+__global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
+                               const int2* __restrict__ tiles, int ntiles, int to_temp, unsigned* status) {
+  const double C1 = 3.0 / 2.56e2, C2 = -2.5e1 / 2.56e2, C3 = 7.5e1 / 1.28e2;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBox& bx = boxes[tile.x];
+    const int p = tile.y + threadIdx.x;
+    const int np = bx.n[0] * bx.n[1] * bx.n[2];
+    if (p >= np) continue;
+    const int c[3] = {bx.lo[0] + p % bx.n[0], bx.lo[1] + (p / bx.n[0]) % bx.n[1], bx.lo[2] + p / (bx.n[0] * bx.n[1])};
+    const AmrBlock& D = blocks[bx.dst];
+    const AmrBlock& S = blocks[bx.src];
+    const int f0[3] = {2 * c[0] - 2, 2 * c[1] - 2, 2 * c[2] - 2};
+    if (!amr_inside(D, c[0], c[1], c[2]) || !amr_inside(S, f0[0], f0[1], f0[2]) ||
+        !amr_inside(S, f0[0] + 5, f0[1] + 5, f0[2] + 5)) {
+      atomicOr(status, ST_BAD_ARG);
+      continue;
+    }
+    const double* src = amr_state(S);
+    const long long sy = S.ex[0], sz = (long long)S.ex[0] * S.ex[1];
+    const long long base = amr_idx(S, f0[0], f0[1], f0[2]);
+    double out[24];
+    for (int f = 0; f < 24; ++f) {
+      const double* q = src + f * S.fs + base;
+      double tmp1[6];
+      for (int a = 0; a < 6; ++a) {
+        double t2[6];
+        for (int b = 0; b < 6; ++b) {
+          const double* r = q + a + b * sy;
+          t2[b] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(r[0], r[5 * sz])), __dmul_rn(C2, __dadd_rn(r[sz], r[4 * sz]))),
+                            __dmul_rn(C3, __dadd_rn(r[2 * sz], r[3 * sz])));
+        }
+        tmp1[a] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(t2[0], t2[5])), __dmul_rn(C2, __dadd_rn(t2[1], t2[4]))),
+                            __dmul_rn(C3, __dadd_rn(t2[2], t2[3])));
+      }
+      out[f] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(tmp1[0], tmp1[5])), __dmul_rn(C2, __dadd_rn(tmp1[1], tmp1[4]))),
+                         __dmul_rn(C3, __dadd_rn(tmp1[2], tmp1[3])));
+    }
+    const long long od = amr_idx(D, c[0], c[1], c[2]);
+    if (to_temp) {
+      for (int f = 0; f < 24; ++f) D.K[f * D.fs + od] = out[f];
+    } else {
+      double* dst = amr_state(D);
+      for (int f = 0; f < 24; ++f) dst[f * D.fs + od] = out[f];
+    }
+  }
+}
+
+// Parent state at the child's intermediate time into K (prepare_inter_time_level,
+// Parallel.C:4329-4441): average2 (fmisc.f90:1569-1592, 3/8 new + 3/4 old
+// - 1/8 older) once the level has two steps behind it, else average
+// (fmisc.f90:1532, (new + old)/2).  One thread per block point.
+__global__ void k_amr_timeinterp(const AmrBlock* __restrict__ blocks, const int2* __restrict__ tiles, int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBlock& B = blocks[tile.x];
+    const long long p = (long long)tile.y + threadIdx.x;
+    const long long np = (long long)B.ex[0] * B.ex[1] * B.ex[2];
+    if (p >= np) continue;
+    const int cur = B.lvl[0];
+    const double* f1 = B.tl[cur];
+    const double* f2 = B.tl[(cur + 2) % 3];
+    const double* f3 = B.tl[(cur + 1) % 3];
+    if (B.lvl[1] >= 2) {
+      const double C1 = 3.0 / 8.0, C2 = 3.0 / 4.0, C3 = -1.0 / 8.0;
+      for (int f = 0; f < 24; ++f) {
+        const long long o = f * B.fs + p;
+        B.K[o] = __dadd_rn(__dadd_rn(__dmul_rn(C1, f1[o]), __dmul_rn(C2, f2[o])), __dmul_rn(C3, f3[o]));
+      }
+    } else {
+      for (int f = 0; f < 24; ++f) {
+        const long long o = f * B.fs + p;
+        B.K[o] = __dmul_rn(0.5, __dadd_rn(f1[o], f2[o]));
+      }
+    }
+  }
+}
+
+// enforce_ga in place on the current state of every block of a level, as the
+// reference does on StateList at the start of each level step
+// (bssn_class.C:3052).  One thread per block point.
+__global__ void k_amr_enforce(const AmrBlock* __restrict__ blocks, const int2* __restrict__ tiles, int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBlock& B = blocks[tile.x];
+    const long long p = (long long)tile.y + threadIdx.x;
+    const long long np = (long long)B.ex[0] * B.ex[1] * B.ex[2];
+    if (p >= np) continue;
+    double* u = B.tl[B.lvl[0]];
+    double g[6], a[6];
+    for (int m = 0; m < 6; ++m) { g[m] = u[(F_GXX + m) * B.fs + p]; a[m] = u[(F_AXX + m) * B.fs + p]; }
+    enforce_ga_point(g, a);
+    for (int m = 0; m < 6; ++m) { u[(F_GXX + m) * B.fs + p] = g[m]; u[(F_AXX + m) * B.fs + p] = a[m]; }
+  }
+}
+
+// Advance a level's time-level ring and step counter.
+__global__ void k_amr_rotate(int* lvl) {
+  lvl[0] = (lvl[0] + 1) % 3;
+  lvl[1] = lvl[1] + 1;
+}
+
+}  // namespace amss

@@ -1,0 +1,28 @@
+// amr_types.cuh -- host/device descriptors of the AMR data movement (amr.cuh).
+#pragma once
+#include "bssn_step.cuh"
+
+namespace amss {
+
+// Per-block buffers as the AMR kernels see them (one table for all levels).
+struct AmrBlock {
+  int org[3];          // global level index of array element 0
+  int ex[3];
+  long long fs;
+  double* tl[3];       // three time levels of the FP64 state; tl[cur] is current
+  void* st[2];         // stage buffers (FP64, or FP32 in the mixed form)
+  double* side[2];     // FP64 chi, alpha of the stages (mixed form)
+  double* K;           // RK accumulator, reused as the time-interpolated parent state
+  const int* lvl;      // level state {cur, steps taken}
+};
+
+// A box of work: [lo, lo + n) in global level indices of the destination.
+struct AmrBox {
+  int dst, src;        // block ids
+  int lo[3];
+  int n[3];
+};
+
+enum AmrBuf : int { BUF_STATE = 0, BUF_STAGE_A = 1, BUF_STAGE_B = 2, BUF_TEMP = 3 };
+
+}  // namespace amss

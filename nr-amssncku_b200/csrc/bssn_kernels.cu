@@ -27,16 +27,18 @@ namespace amss {
 __global__ void k_rk4(long long n, double dT, const double* __restrict__ f0, double* f1, double* f_rhs, int RK4) {
   const double F1o6 = 1.0 / 6.0, HLF = 0.5, TWO = 2.0;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    // explicitly rounded operations (no FMA contraction): the same IEEE
+    // operations, in the same order, as the Fortran
     if (RK4 == 0) {
-      f1[p] = f0[p] + HLF * dT * f_rhs[p];
+      f1[p] = __dadd_rn(f0[p], __dmul_rn(__dmul_rn(HLF, dT), f_rhs[p]));
     } else if (RK4 == 1) {
-      f_rhs[p] = f_rhs[p] + TWO * f1[p];
-      f1[p] = f0[p] + HLF * dT * f1[p];
+      f_rhs[p] = __dadd_rn(f_rhs[p], __dmul_rn(TWO, f1[p]));
+      f1[p] = __dadd_rn(f0[p], __dmul_rn(__dmul_rn(HLF, dT), f1[p]));
     } else if (RK4 == 2) {
-      f_rhs[p] = f_rhs[p] + TWO * f1[p];
-      f1[p] = f0[p] + dT * f1[p];
+      f_rhs[p] = __dadd_rn(f_rhs[p], __dmul_rn(TWO, f1[p]));
+      f1[p] = __dadd_rn(f0[p], __dmul_rn(dT, f1[p]));
     } else {
-      f1[p] = f0[p] + F1o6 * dT * (f1[p] + f_rhs[p]);
+      f1[p] = __dadd_rn(f0[p], __dmul_rn(__dmul_rn(F1o6, dT), __dadd_rn(f1[p], f_rhs[p])));
     }
   }
 }
@@ -271,7 +273,9 @@ extern "C" int compute_rhs_bssn_(
     const double bb[6] = {X[0], Y[0], Z[0], X[ex[0] - 1], Y[ex[1] - 1], Z[ex[2] - 1]};
     block_faces(ex, X, Y, Z, bb, *Symmetry, &b.face_mask, &b.lowsym_mask);
   }
-  const Coef<double> C = make_coef<double>(b.dx, *eps);
+  Coefs<double> C;
+  C.t = make_coef<double>(b.dx, *eps);
+  C.d = C.t;
   RhsAux aux{dg, dR, dc, dm, fs, *co};
   const int grid = grid_for(n, 128);
   if (b.lowsym_mask) AMSS_CK(launch_rhs_dropin<true>(grid, s, b, C, du, dr, aux, c.dstatus));

@@ -59,16 +59,29 @@ __device__ __forceinline__ PointGates point_gates(const BlockView& b, int i, int
 // Finish one field: + lopsided (x, y, z) + KO, then hand it to the epilogue.
 // `add1` = 1 for the diagonal metric (advected as g = d + 1, bssn_rhs.f90:948-953).
 template <typename T, int F, typename P, typename E>
-__device__ __forceinline__ void finish_field(const P& q, const Coef<T>& C, const PointGates& g, T r, T bx, T by,
+__device__ __forceinline__ void finish_field(const P& q, const Coefs<T>& C, const PointGates& g, T r, T bx, T by,
                                              T bz, T add1, E& epi) {
+  if constexpr (P::kPre) {
+    // split form: the stencil pass stored the advection sum and the KO line sum
+    if (g.lop) r = r + q.template dv<T>(doff(F) + dslots(F) - 2);
+    if (g.ko) r = r + pick<T>(C).ko * q.template dv<T>(doff(F) + dslots(F) - 1);
+    epi.template put<F>(r);
+    return;
+  }
   if (g.lop) {
     r = lop_dir<T, F, 0>(q, C, r, bx, q.i, g.lo3[0], g.hi[0], add1);
     r = lop_dir<T, F, 1>(q, C, r, by, q.j, g.lo3[1], g.hi[1], add1);
     r = lop_dir<T, F, 2>(q, C, r, bz, q.k, g.lo3[2], g.hi[2], add1);
   }
   if (g.ko) {
-    r = r + C.ko * (divh(ko_line<T, F, 0>(q), C.h[0]) + divh(ko_line<T, F, 1>(q), C.h[1]) +
-                    divh(ko_line<T, F, 2>(q), C.h[2]));
+    using A = std::conditional_t<wide_field<F>(), double, T>;
+    const Coef<A>& c = pick<A>(C);
+    if constexpr (std::is_same_v<A, T>)
+      r = r + c.ko * (divh(ko_line<A, F, 0>(q), c.h[0]) + divh(ko_line<A, F, 1>(q), c.h[1]) +
+                      divh(ko_line<A, F, 2>(q), c.h[2]));
+    else
+      r = r + (T)(c.ko * (divh(ko_line<A, F, 0>(q), c.h[0]) + divh(ko_line<A, F, 1>(q), c.h[1]) +
+                          divh(ko_line<A, F, 2>(q), c.h[2])));
   }
   epi.template put<F>(r);
 }
@@ -85,17 +98,20 @@ __device__ __forceinline__ unsigned nan_bits(const T* v, int n) {
   return s;
 }
 
-template <typename T, typename SI, bool SYMM, bool AUX, typename E>
-__device__ __forceinline__ unsigned bssn_rhs_point(const Pt<SI, SYMM>& q, const Coef<T>& C, const PointGates& G,
+template <typename T, typename SI, bool SYMM, bool AUX, typename E, typename P>
+__device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C, const PointGates& G,
                                                    const RhsAux& aux, E& epi) {
+  static_assert(!(AUX && P::kPre), "the diagnostic outputs need the stencil accessor");
   const T ZEO = T(0), ONE = T(1), TWO = T(2), FOUR = T(4), EIGHT = T(8), HALF = T(0.5);
   const T FF = T(0.75), eta = T(2);
   const T F1o3 = T(1.0 / 3.0), F2o3 = T(2.0 / 3.0), F3o2 = T(1.5);
   const T PI = T(3.141592653589793238462643383279502884);
   const int ord = G.ord;
 
-  // centre values
-  const T chi = q.template v<T, F_CHI>(0, 0, 0), trK = q.template v<T, F_TRK>(0, 0, 0);
+  // centre values; chi and alpha are read and shifted in FP64 (chi -> 0 near a
+  // puncture, so chi+1 must be formed before rounding to T)
+  const double chi64 = q.template v<double, F_CHI>(0, 0, 0), Lap64 = q.template v<double, F_LAP>(0, 0, 0);
+  const T chi = (T)chi64, trK = q.template v<T, F_TRK>(0, 0, 0);
   const T dxx = q.template v<T, F_GXX>(0, 0, 0), gxy = q.template v<T, F_GXY>(0, 0, 0);
   const T gxz = q.template v<T, F_GXZ>(0, 0, 0), dyy = q.template v<T, F_GYY>(0, 0, 0);
   const T gyz = q.template v<T, F_GYZ>(0, 0, 0), dzz = q.template v<T, F_GZZ>(0, 0, 0);
@@ -103,7 +119,7 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const Pt<SI, SYMM>& q, const 
   const T Axz = q.template v<T, F_AXZ>(0, 0, 0), Ayy = q.template v<T, F_AYY>(0, 0, 0);
   const T Ayz = q.template v<T, F_AYZ>(0, 0, 0), Azz = q.template v<T, F_AZZ>(0, 0, 0);
   const T Gamx = q.template v<T, F_GAMX>(0, 0, 0), Gamy = q.template v<T, F_GAMY>(0, 0, 0);
-  const T Gamz = q.template v<T, F_GAMZ>(0, 0, 0), Lap = q.template v<T, F_LAP>(0, 0, 0);
+  const T Gamz = q.template v<T, F_GAMZ>(0, 0, 0), Lap = (T)Lap64;
   const T betax = q.template v<T, F_BETAX>(0, 0, 0), betay = q.template v<T, F_BETAY>(0, 0, 0);
   const T betaz = q.template v<T, F_BETAZ>(0, 0, 0);
   const T dtSfx = q.template v<T, F_DTSFX>(0, 0, 0), dtSfy = q.template v<T, F_DTSFY>(0, 0, 0);
@@ -126,7 +142,7 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const Pt<SI, SYMM>& q, const 
     }
   }
 
-  const T alpn1 = Lap + ONE, chin1 = chi + ONE;
+  const T alpn1 = (T)(Lap64 + 1.0), chin1 = (T)(chi64 + 1.0);
   const T gxx = dxx + ONE, gyy = dyy + ONE, gzz = dzz + ONE;
 
   // :152-160

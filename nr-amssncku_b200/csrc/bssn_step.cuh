@@ -9,11 +9,13 @@
 //   stage input --stencils--> RHS k --RK4 update--> face rule --> chi floor
 //   --> enforce_ga --> stage output
 //
-// enforce_ga is applied to what a substep writes rather than to what the next
-// one reads.  It is pointwise, so enforce_ga(floor(rk(x))) at a point equals
-// the reference's "write, then enforce in place before the next RHS"; the one
-// visible difference is that the state stored after a full step is already
-// in the enforced form the reference gives it at the start of the next step.
+// enforce_ga of the stage outputs of substeps 0-2 is applied as they are
+// written rather than by a pass before the next substep reads them: it is
+// pointwise, so enforce_ga(floor(rk(x))) at a point equals the reference's
+// "write, then enforce in place before the next RHS".  The new state written
+// by substep 3 is left as the reference leaves it; the engine enforces it in
+// place at the start of the next step, after the AMR transfers have run, as
+// the reference does.
 #pragma once
 #include "bssn_rhs.cuh"
 
@@ -69,6 +71,7 @@ struct EpiRK {
   const double* u0;   // state at t_n (FP64)
   double* K;          // RK accumulator (FP64)
   SO* out;            // stage output, or the new state at sub == 3
+  double* out_side;   // FP64 chi, alpha of an FP32 stage output
   long long fs, p;
   int sub;
   bool freeze;        // outer face of a refined patch: output = u0 there
@@ -110,6 +113,7 @@ struct EpiRK {
     else if constexpr (F == F_AYY) a[3] = r;
     else if constexpr (F == F_AYZ) a[4] = r;
     else if constexpr (F == F_AZZ) a[5] = r;
+    else if constexpr (sizeof(SO) == 4 && wide_field<F>()) out_side[side_slot(F) * fs + p] = r;
     else out[o] = (SO)r;
   }
   __device__ __forceinline__ void finish() {
@@ -157,12 +161,15 @@ __device__ __forceinline__ T sommerfeld_point(const P& q, const T (&d2)[3], cons
 template <typename T>
 struct StepBlock {
   BlockView b;
-  Coef<T> C;
+  Coefs<T> C;
   T d2s[3];           // 1/2/dx for the Sommerfeld rule
-  double* u0;         // state at t_n (FP64)
+  double* tl[3];      // three time levels of the FP64 state: tl[cur] = U0 (t_n),
+                      // tl[(cur+1)%3] receives U_new (it held t_n - 2 dt)
+  const int* lvl;     // level state {cur, steps taken} (device, rotated after each step)
   void* stage[2];     // stage buffers A and B (type of the stage storage)
+  double* side[2];    // FP64 chi, alpha of stages A and B (mixed form only)
   double* K;          // RK accumulator (FP64)
-  double* unew;       // new state, may equal u0
+  long long doff;     // offset of this block's points in the level's D slots (split form)
   long long npts;
   int lev0;           // 1: Sommerfeld rule on the patch faces; 0: freeze them at u0
 };

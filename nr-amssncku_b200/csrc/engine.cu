@@ -1,12 +1,19 @@
 // engine.cu -- the batched, device-resident evolution engine (amss_engine_*).
 //
-// All blocks live in one HBM arena.  Per block: the FP64 state U0, two stage
-// buffers (FP64, or FP32 in the mixed form), the FP64 RK accumulator K and
-// the coordinate arrays.  Per level: a table of StepBlock descriptors and a
-// tile list (128 points per tile, tiles never straddle blocks), so one
-// persistent launch advances every block of the level, whatever their sizes,
-// by one RK4 substep.  Four launches make a step; a step (or many) can be
-// captured once as a CUDA graph and replayed.
+// All blocks live in one HBM arena.  Per block: three time levels of the FP64
+// state (a ring: current, previous, the one before -- what the reference keeps
+// as StateList / OldStateList / SynchList_cor after its rotation,
+// bssn_class.C:3852-3853), two stage buffers (FP64, or FP32 plus FP64 chi and
+// alpha in the mixed form), the FP64 RK accumulator K and the coordinates.
+// The ring is advanced by a one-thread kernel that bumps a per-level index in
+// device memory, so kernel arguments never change and a whole Berger-Oliger
+// coarse step can be captured once as a CUDA graph and replayed.
+//
+// Per level: a table of StepBlock descriptors and a tile list (128 points per
+// tile, tiles never straddle blocks) so one launch advances every block of the
+// level by one RK4 substep; box lists for the same-level ghost sync and, for
+// refined levels, for restriction into and prolongation from the parent.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,7 +21,8 @@
 #include <string>
 #include <vector>
 
-#include "bssn_step.cuh"
+#include "amr_types.cuh"
+#include "deriv.cuh"
 #include "dev_util.cuh"
 
 namespace amss {
@@ -23,10 +31,22 @@ template <typename T>
 Coef<T> make_coef(const double dx[3], double eps);
 void block_faces(const int ex[3], const double* X, const double* Y, const double* Z, const double bbox[6],
                  int symmetry, int* face_mask, int* lowsym_mask);
-template <typename T, typename SS, bool SYMM>
+template <typename T, typename SS, bool SYMM, bool SPLIT>
 cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, int sub, RKConst rk, int enforce,
-                           unsigned* status, int grid, cudaStream_t s);
+                           unsigned* status, int grid, cudaStream_t s, const void* D, long long dfs);
+template <typename T, typename SS>
+cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
+                         int grid, cudaStream_t s);
 cudaError_t launch_enforce(long long n, long long fs, double* g, double* a, cudaStream_t s);
+cudaError_t launch_amr_sync(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles, int which,
+                            bool fp32_stages, unsigned* status, cudaStream_t s);
+cudaError_t launch_amr_prolong(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
+                               int from_temp, unsigned* status, cudaStream_t s);
+cudaError_t launch_amr_restrict(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
+                                int to_temp, unsigned* status, cudaStream_t s);
+cudaError_t launch_amr_timeinterp(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
+cudaError_t launch_amr_rotate(int* lvl, cudaStream_t s);
+cudaError_t launch_amr_enforce(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
 
 static thread_local std::string g_err;
 
@@ -41,8 +61,7 @@ int check_device(const char* who) {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {
     char m[256];
-    std::snprintf(m, sizeof m,
-                  "%s: no usable CUDA device (%s); the B200 kernels have no CPU fallback", who,
+    std::snprintf(m, sizeof m, "%s: no usable CUDA device (%s); the B200 kernels have no CPU fallback", who,
                   e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
     amss_fail(AMSS_ERR_NO_DEVICE, m);
     return -1;
@@ -50,25 +69,78 @@ int check_device(const char* who) {
   return 0;
 }
 
-struct EBlock {
+struct Box {
+  int lo[3], hi[3];
+  bool empty() const { return lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2]; }
+};
+static Box intersect(const Box& a, const Box& b) {
+  Box r;
+  for (int d = 0; d < 3; ++d) {
+    r.lo[d] = std::max(a.lo[d], b.lo[d]);
+    r.hi[d] = std::min(a.hi[d], b.hi[d]);
+  }
+  return r;
+}
+
+struct EPatch {
   int level;
-  int ex[3];
-  double bbox[6], pbbox[6];
+  Box phys;            // physical cells
+  int buffer;          // buffer cells each side (0 on level 0)
+  Box ext() const {
+    Box b = phys;
+    for (int d = 0; d < 3; ++d) { b.lo[d] -= buffer; b.hi[d] += buffer; }
+    return b;
+  }
+  std::vector<int> blocks;
+};
+
+struct EBlock {
+  int level = 0, patch = -1;
+  int ex[3], org[3];
+  Box own;
   long long npts, fs;
+  double bbox[6], pbbox[6];
   std::vector<double> X, Y, Z;
   int face_mask = 0, lowsym = 0;
   double* dX = nullptr;
-  double* u0 = nullptr;
-  void* st[2] = {nullptr, nullptr};
+  double* tl[3] = {nullptr, nullptr, nullptr};
   double* K = nullptr;
+  void* st[2] = {nullptr, nullptr};
+  double* side[2] = {nullptr, nullptr};
+  Box array() const {
+    Box b;
+    for (int d = 0; d < 3; ++d) { b.lo[d] = org[d]; b.hi[d] = org[d] + ex[d]; }
+    return b;
+  }
+};
+
+struct DevBoxes {
+  AmrBox* boxes = nullptr;
+  int2* tiles = nullptr;
+  int ntiles = 0;
+  void release() {
+    if (boxes) cudaFree(boxes);
+    if (tiles) cudaFree(tiles);
+    boxes = nullptr;
+    tiles = nullptr;
+  }
 };
 
 struct ELevel {
   std::vector<int> blocks;
+  std::vector<int> patches;
   int ntiles = 0;
-  int2* dtiles = nullptr;
-  void* dtable = nullptr;
+  int2* dtiles = nullptr;       // substep tiles (index into this level's table)
+  void* dtable = nullptr;       // StepBlock table
   bool symm = false;
+  DevBoxes sync, restrict_, prolong;
+  int2* dti_tiles = nullptr;    // time-interpolation tiles (global block ids)
+  int nti = 0;
+  DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
+  int nditems = 0;
+  long long dfs = 0;            // slot stride of D for this level
+  int cur = 0;                  // host mirror of the ring index
+  long long steps = 0;
 };
 
 }  // namespace amss
@@ -77,10 +149,18 @@ using namespace amss;
 
 struct amss_engine {
   amss_params prm;
+  bool grid_set = false;
+  double x0[3] = {0, 0, 0};
+  double h0 = 1.0;
   std::vector<EBlock> blocks;
+  std::vector<EPatch> patches;
+  std::map<std::pair<int, int>, int> patch_ids;   // (level, patch) -> index
   std::map<int, ELevel> levels;
   cudaStream_t stream = nullptr;
   unsigned* dstatus = nullptr;
+  int* dlvl = nullptr;          // 2 ints per level: ring index, steps taken
+  AmrBlock* dblocks = nullptr;
+  void* D = nullptr;            // stencil terms of the level being stepped (split form)
   char* arena = nullptr;
   size_t arena_bytes = 0;
   long long launches = 0;
@@ -89,7 +169,7 @@ struct amss_engine {
 };
 
 extern "C" const char* amss_last_error(void) { return g_err.c_str(); }
-extern "C" const char* amss_version(void) { return "amss_b200 0.1 (sm_100a)"; }
+extern "C" const char* amss_version(void) { return "amss_b200 0.2 (sm_100a)"; }
 
 extern "C" amss_engine* amss_engine_create(const amss_params* prm) {
   if (!prm) { amss_fail(AMSS_ERR_ARG, "amss_engine_create: null params"); return nullptr; }
@@ -113,13 +193,35 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
   if (!e) return;
   if (e->stream) cudaStreamSynchronize(e->stream);
   for (auto& kv : e->levels) {
-    if (kv.second.dtiles) cudaFree(kv.second.dtiles);
-    if (kv.second.dtable) cudaFree(kv.second.dtable);
+    ELevel& L = kv.second;
+    if (L.dtiles) cudaFree(L.dtiles);
+    if (L.dtable) cudaFree(L.dtable);
+    if (L.dti_tiles) cudaFree(L.dti_tiles);
+    if (L.ditems) cudaFree(L.ditems);
+    L.sync.release();
+    L.restrict_.release();
+    L.prolong.release();
   }
+  if (e->dblocks) cudaFree(e->dblocks);
+  if (e->D) cudaFree(e->D);
+  if (e->dlvl) cudaFree(e->dlvl);
   if (e->arena) cudaFree(e->arena);
   if (e->dstatus) cudaFree(e->dstatus);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
+}
+
+static void finish_block(amss_engine* e, EBlock& b, const double bbox[6], const double pbbox[6]) {
+  for (int m = 0; m < 6; ++m) { b.bbox[m] = bbox[m]; b.pbbox[m] = pbbox[m]; }
+  b.npts = (long long)b.ex[0] * b.ex[1] * b.ex[2];
+  b.fs = pad_stride(b.npts);
+  std::vector<double>* xs[3] = {&b.X, &b.Y, &b.Z};
+  for (int d = 0; d < 3; ++d) {  // Block.C:48-52 (Cell)
+    const double h = (bbox[3 + d] - bbox[d]) / b.ex[d];
+    xs[d]->resize(b.ex[d]);
+    for (int j = 0; j < b.ex[d]; ++j) (*xs[d])[j] = bbox[d] + (j + 0.5) * h;
+  }
+  block_faces(b.ex, b.X.data(), b.Y.data(), b.Z.data(), b.pbbox, e->prm.symmetry, &b.face_mask, &b.lowsym);
 }
 
 extern "C" int amss_engine_add_block(amss_engine* e, int level, const int ex[3], const double bbox[6],
@@ -128,17 +230,79 @@ extern "C" int amss_engine_add_block(amss_engine* e, int level, const int ex[3],
   if (ex[0] < 7 || ex[1] < 7 || ex[2] < 7) return amss_fail(AMSS_ERR_ARG, "amss_engine_add_block: ex < 7");
   EBlock b;
   b.level = level;
-  for (int d = 0; d < 3; ++d) b.ex[d] = ex[d];
-  for (int m = 0; m < 6; ++m) { b.bbox[m] = bbox[m]; b.pbbox[m] = patch_bbox[m]; }
-  b.npts = (long long)ex[0] * ex[1] * ex[2];
-  b.fs = pad_stride(b.npts);
-  std::vector<double>* xs[3] = {&b.X, &b.Y, &b.Z};
-  for (int d = 0; d < 3; ++d) {  // Block.C:48-52 (Cell)
-    const double h = (bbox[3 + d] - bbox[d]) / ex[d];
-    xs[d]->resize(ex[d]);
-    for (int j = 0; j < ex[d]; ++j) (*xs[d])[j] = bbox[d] + (j + 0.5) * h;
+  for (int d = 0; d < 3; ++d) {
+    b.ex[d] = ex[d];
+    b.org[d] = 0;
+    b.own.lo[d] = 0;
+    b.own.hi[d] = ex[d];
   }
-  block_faces(b.ex, b.X.data(), b.Y.data(), b.Z.data(), b.pbbox, e->prm.symmetry, &b.face_mask, &b.lowsym);
+  EPatch p;
+  p.level = level;
+  p.phys = b.own;
+  p.buffer = 0;
+  const int pid = (int)e->patches.size();
+  p.blocks.push_back((int)e->blocks.size());
+  e->patches.push_back(p);
+  b.patch = pid;
+  finish_block(e, b, bbox, patch_bbox);
+  e->blocks.push_back(b);
+  e->levels[level].blocks.push_back((int)e->blocks.size() - 1);
+  e->levels[level].patches.push_back(pid);
+  return (int)e->blocks.size() - 1;
+}
+
+extern "C" int amss_engine_set_grid(amss_engine* e, const double x0[3], double h0) {
+  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_set_grid: engine already committed");
+  if (!(h0 > 0)) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_grid: h0 must be > 0");
+  for (int d = 0; d < 3; ++d) e->x0[d] = x0[d];
+  e->h0 = h0;
+  e->grid_set = true;
+  return 0;
+}
+
+extern "C" int amss_engine_add_amr_block(amss_engine* e, int level, int patch, const int org[3], const int ex[3],
+                                         const int own_lo[3], const int own_hi[3], const int phys_lo[3],
+                                         const int phys_hi[3], int buffer) {
+  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_add_amr_block: engine already committed");
+  if (!e->grid_set) return amss_fail(AMSS_ERR_STATE, "amss_engine_add_amr_block: call amss_engine_set_grid first");
+  if (level < 0 || level > 30 || buffer < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_add_amr_block: bad level/buffer");
+  EBlock b;
+  b.level = level;
+  for (int d = 0; d < 3; ++d) {
+    b.ex[d] = ex[d];
+    b.org[d] = org[d];
+    b.own.lo[d] = own_lo[d];
+    b.own.hi[d] = own_hi[d];
+    if (ex[d] < 7 || own_lo[d] < org[d] || own_hi[d] > org[d] + ex[d] || own_lo[d] >= own_hi[d])
+      return amss_fail(AMSS_ERR_ARG, "amss_engine_add_amr_block: owned box must lie in the array, ex >= 7");
+  }
+  const auto key = std::make_pair(level, patch);
+  auto it = e->patch_ids.find(key);
+  int pid;
+  if (it == e->patch_ids.end()) {
+    EPatch p;
+    p.level = level;
+    for (int d = 0; d < 3; ++d) { p.phys.lo[d] = phys_lo[d]; p.phys.hi[d] = phys_hi[d]; }
+    p.buffer = buffer;
+    pid = (int)e->patches.size();
+    e->patches.push_back(p);
+    e->patch_ids[key] = pid;
+    e->levels[level].patches.push_back(pid);
+  } else {
+    pid = it->second;
+  }
+  b.patch = pid;
+  const double h = e->h0 / std::ldexp(1.0, level);
+  const Box ext = e->patches[pid].ext();
+  double bbox[6], pbbox[6];
+  for (int d = 0; d < 3; ++d) {
+    bbox[d] = e->x0[d] + org[d] * h;
+    bbox[3 + d] = e->x0[d] + (org[d] + ex[d]) * h;
+    pbbox[d] = e->x0[d] + ext.lo[d] * h;
+    pbbox[3 + d] = e->x0[d] + ext.hi[d] * h;
+  }
+  finish_block(e, b, bbox, pbbox);
+  e->patches[pid].blocks.push_back((int)e->blocks.size());
   e->blocks.push_back(b);
   e->levels[level].blocks.push_back((int)e->blocks.size() - 1);
   return (int)e->blocks.size() - 1;
@@ -148,9 +312,16 @@ template <typename T>
 static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<StepBlock<T>> tab;
   std::vector<int2> tiles;
+  std::vector<DerivItem> items;
+  long long doff = 0;
   for (size_t m = 0; m < L.blocks.size(); ++m) {
     EBlock& b = e->blocks[L.blocks[m]];
     StepBlock<T> s{};
+    s.doff = doff;
+    doff += b.fs;
+    for (int y0 = 0; y0 < b.ex[1]; y0 += DTY)
+      for (int x0 = 0; x0 < b.ex[0]; x0 += DTX)
+        for (int f = 0; f < 24; ++f) items.push_back(DerivItem{(int)m, x0, y0, f});
     s.b.ex[0] = b.ex[0]; s.b.ex[1] = b.ex[1]; s.b.ex[2] = b.ex[2];
     s.b.fs = b.fs;
     s.b.X = b.dX; s.b.Y = b.dX + b.ex[0]; s.b.Z = b.dX + b.ex[0] + b.ex[1];
@@ -158,13 +329,16 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     s.b.face_mask = b.face_mask;
     s.b.symmetry = e->prm.symmetry;
     s.b.lowsym_mask = b.lowsym;
-    s.C = make_coef<T>(s.b.dx, e->prm.eps);
+    s.C.t = make_coef<T>(s.b.dx, e->prm.eps);
+    s.C.d = make_coef<double>(s.b.dx, e->prm.eps);
     for (int d = 0; d < 3; ++d) s.d2s[d] = (T)(1.0 / 2.0 / s.b.dx[d]);
-    s.u0 = b.u0;
+    for (int t = 0; t < 3; ++t) s.tl[t] = b.tl[t];
+    s.lvl = e->dlvl + 2 * level;
     s.stage[0] = b.st[0];
     s.stage[1] = b.st[1];
+    s.side[0] = b.side[0];
+    s.side[1] = b.side[1];
     s.K = b.K;
-    s.unew = b.u0;
     s.npts = b.npts;
     s.lev0 = level == 0 ? 1 : 0;
     if (b.lowsym) L.symm = true;
@@ -172,6 +346,10 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     for (long long p = 0; p < b.npts; p += 128) tiles.push_back(make_int2((int)m, (int)p));
   }
   L.ntiles = (int)tiles.size();
+  L.dfs = doff;
+  L.nditems = (int)items.size();
+  AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
+  AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   AMSS_CK(cudaMalloc(&L.dtable, tab.size() * sizeof(StepBlock<T>)));
   AMSS_CK(cudaMemcpy(L.dtable, tab.data(), tab.size() * sizeof(StepBlock<T>), cudaMemcpyHostToDevice));
   AMSS_CK(cudaMalloc(&L.dtiles, tiles.size() * sizeof(int2)));
@@ -179,16 +357,111 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   return 0;
 }
 
+static int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D) {
+  std::vector<int2> tiles;
+  for (size_t m = 0; m < boxes.size(); ++m) {
+    const long long n = (long long)boxes[m].n[0] * boxes[m].n[1] * boxes[m].n[2];
+    for (long long p = 0; p < n; p += 128) tiles.push_back(make_int2((int)m, (int)p));
+  }
+  D.ntiles = (int)tiles.size();
+  if (boxes.empty()) return 0;
+  AMSS_CK(cudaMalloc(&D.boxes, boxes.size() * sizeof(AmrBox)));
+  AMSS_CK(cudaMemcpy(D.boxes, boxes.data(), boxes.size() * sizeof(AmrBox), cudaMemcpyHostToDevice));
+  AMSS_CK(cudaMalloc(&D.tiles, tiles.size() * sizeof(int2)));
+  AMSS_CK(cudaMemcpy(D.tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static void push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b) {
+  if (b.empty()) return;
+  AmrBox a;
+  a.dst = dst;
+  a.src = src;
+  for (int d = 0; d < 3; ++d) { a.lo[d] = b.lo[d]; a.n[d] = b.hi[d] - b.lo[d]; }
+  v.push_back(a);
+}
+
+// Same-level ghost fill (Parallel::Sync, Parallel.C:3677-3776): every cell of a
+// block's array that another block of the level owns is copied from it.
+static std::vector<AmrBox> sync_boxes(amss_engine* e, const ELevel& L) {
+  std::vector<AmrBox> v;
+  for (int d : L.blocks)
+    for (int s : L.blocks)
+      if (d != s) push_box(v, d, s, intersect(e->blocks[d].array(), e->blocks[s].own));
+  return v;
+}
+
+// Restriction (Parallel::Restrict, Parallel.C:4485-4543): every cell of a
+// parent block's array (ghosts included) inside a child patch's physical
+// region, from the child block that owns its two children per direction.
+static std::vector<AmrBox> restrict_boxes(amss_engine* e, const ELevel& F, const ELevel& C) {
+  std::vector<AmrBox> v;
+  for (int pid : F.patches) {
+    const EPatch& P = e->patches[pid];
+    Box cphys;
+    for (int d = 0; d < 3; ++d) { cphys.lo[d] = P.phys.lo[d] / 2; cphys.hi[d] = P.phys.hi[d] / 2; }
+    for (int cb : C.blocks) {
+      const Box r = intersect(cphys, e->blocks[cb].array());
+      if (r.empty()) continue;
+      for (int fb : P.blocks) {
+        const Box& o = e->blocks[fb].own;
+        Box oc;
+        for (int d = 0; d < 3; ++d) { oc.lo[d] = o.lo[d] / 2; oc.hi[d] = o.hi[d] / 2; }
+        push_box(v, cb, fb, intersect(r, oc));
+      }
+    }
+  }
+  return v;
+}
+
+// Prolongation into the buffer cells (Parallel::OutBdLow2Hi,
+// Parallel.C:4589-4689): every cell of a child block's array in its patch's
+// buffer region, from the parent block that owns the cell's parent.
+static std::vector<AmrBox> prolong_boxes(amss_engine* e, const ELevel& F, const ELevel& C) {
+  std::vector<AmrBox> v;
+  for (int pid : F.patches) {
+    const EPatch& P = e->patches[pid];
+    const Box ext = P.ext();
+    std::vector<Box> slabs;
+    for (int d = 0; d < 3; ++d) {
+      Box lo = ext, hi = ext;
+      for (int q = 0; q < d; ++q) { lo.lo[q] = hi.lo[q] = P.phys.lo[q]; lo.hi[q] = hi.hi[q] = P.phys.hi[q]; }
+      lo.hi[d] = P.phys.lo[d];
+      hi.lo[d] = P.phys.hi[d];
+      slabs.push_back(lo);
+      slabs.push_back(hi);
+    }
+    for (int fb : P.blocks)
+      for (const Box& s : slabs) {
+        const Box r = intersect(s, e->blocks[fb].array());
+        if (r.empty()) continue;
+        for (int cb : C.blocks) {
+          const Box& o = e->blocks[cb].own;
+          Box of;
+          for (int d = 0; d < 3; ++d) { of.lo[d] = 2 * o.lo[d]; of.hi[d] = 2 * o.hi[d]; }
+          push_box(v, fb, cb, intersect(r, of));
+        }
+      }
+  }
+  return v;
+}
+
 extern "C" int amss_engine_commit(amss_engine* e) {
   if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: already committed");
+  if (e->blocks.empty()) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: no blocks");
   const bool mixed = e->prm.precision == 1;
   const size_t ss = mixed ? sizeof(float) : sizeof(double);
+  int nlev = 0;
+  for (auto& kv : e->levels) nlev = std::max(nlev, kv.first + 1);
+  for (int l = 0; l < nlev; ++l)
+    if (!e->levels.count(l)) return amss_fail(AMSS_ERR_ARG, "amss_engine_commit: levels must be 0..L-1 without gaps");
   size_t bytes = 0;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
   for (auto& b : e->blocks) {
     bytes += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
-    bytes += align((size_t)24 * b.fs * sizeof(double)) * 2;  // u0, K
+    bytes += align((size_t)24 * b.fs * sizeof(double)) * 4;  // 3 time levels + K
     bytes += align((size_t)24 * b.fs * ss) * 2;              // two stages
+    if (mixed) bytes += align((size_t)2 * b.fs * sizeof(double)) * 2;
   }
   AMSS_CK(cudaMalloc(&e->arena, bytes));
   AMSS_CK(cudaMemset(e->arena, 0, bytes));
@@ -197,17 +470,55 @@ extern "C" int amss_engine_commit(amss_engine* e) {
   for (auto& b : e->blocks) {
     b.dX = (double*)p;
     p += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
-    b.u0 = (double*)p; p += align((size_t)24 * b.fs * sizeof(double));
+    for (int t = 0; t < 3; ++t) { b.tl[t] = (double*)p; p += align((size_t)24 * b.fs * sizeof(double)); }
     b.K = (double*)p; p += align((size_t)24 * b.fs * sizeof(double));
     b.st[0] = p; p += align((size_t)24 * b.fs * ss);
     b.st[1] = p; p += align((size_t)24 * b.fs * ss);
+    if (mixed) {
+      b.side[0] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
+      b.side[1] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
+    }
     AMSS_CK(cudaMemcpy(b.dX, b.X.data(), b.ex[0] * sizeof(double), cudaMemcpyHostToDevice));
     AMSS_CK(cudaMemcpy(b.dX + b.ex[0], b.Y.data(), b.ex[1] * sizeof(double), cudaMemcpyHostToDevice));
     AMSS_CK(cudaMemcpy(b.dX + b.ex[0] + b.ex[1], b.Z.data(), b.ex[2] * sizeof(double), cudaMemcpyHostToDevice));
   }
+  AMSS_CK(cudaMalloc(&e->dlvl, sizeof(int) * 2 * nlev));
+  AMSS_CK(cudaMemset(e->dlvl, 0, sizeof(int) * 2 * nlev));
+  std::vector<AmrBlock> ab(e->blocks.size());
+  for (size_t m = 0; m < e->blocks.size(); ++m) {
+    const EBlock& b = e->blocks[m];
+    AmrBlock& a = ab[m];
+    for (int d = 0; d < 3; ++d) { a.org[d] = b.org[d]; a.ex[d] = b.ex[d]; }
+    a.fs = b.fs;
+    for (int t = 0; t < 3; ++t) a.tl[t] = b.tl[t];
+    a.st[0] = b.st[0]; a.st[1] = b.st[1];
+    a.side[0] = b.side[0]; a.side[1] = b.side[1];
+    a.K = b.K;
+    a.lvl = e->dlvl + 2 * b.level;
+  }
+  AMSS_CK(cudaMalloc(&e->dblocks, ab.size() * sizeof(AmrBlock)));
+  AMSS_CK(cudaMemcpy(e->dblocks, ab.data(), ab.size() * sizeof(AmrBlock), cudaMemcpyHostToDevice));
   for (auto& kv : e->levels) {
-    const int rc = mixed ? build_table<float>(e, kv.second, kv.first) : build_table<double>(e, kv.second, kv.first);
+    ELevel& L = kv.second;
+    const int rc = mixed ? build_table<float>(e, L, kv.first) : build_table<double>(e, L, kv.first);
     if (rc) return rc;
+    if (int r2 = upload_boxes(sync_boxes(e, L), L.sync)) return r2;
+    std::vector<int2> ti;
+    for (int b : L.blocks)
+      for (long long q = 0; q < e->blocks[b].npts; q += 128) ti.push_back(make_int2(b, (int)q));
+    L.nti = (int)ti.size();
+    AMSS_CK(cudaMalloc(&L.dti_tiles, ti.size() * sizeof(int2)));
+    AMSS_CK(cudaMemcpy(L.dti_tiles, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if (kv.first > 0) {
+      ELevel& C = e->levels[kv.first - 1];
+      if (int r3 = upload_boxes(restrict_boxes(e, L, C), L.restrict_)) return r3;
+      if (int r4 = upload_boxes(prolong_boxes(e, L, C), L.prolong)) return r4;
+    }
+  }
+  if (e->prm.kernel == 0) {
+    long long mx = 0;
+    for (auto& kv : e->levels) mx = std::max(mx, kv.second.dfs);
+    AMSS_CK(cudaMalloc(&e->D, (size_t)mx * D_SLOTS * (mixed ? sizeof(float) : sizeof(double))));
   }
   e->committed = true;
   return 0;
@@ -219,11 +530,13 @@ static int check_block(amss_engine* e, int block) {
   return 0;
 }
 
+static double* cur_state(amss_engine* e, const EBlock& b) { return b.tl[e->levels[b.level].cur]; }
+
 extern "C" int amss_engine_set_state(amss_engine* e, int block, const double* h) {
   if (int rc = check_block(e, block)) return rc;
   EBlock& b = e->blocks[block];
-  AMSS_CK(cudaMemcpy2DAsync(b.u0, b.fs * sizeof(double), h, b.npts * sizeof(double), b.npts * sizeof(double), 24,
-                            cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(cudaMemcpy2DAsync(cur_state(e, b), b.fs * sizeof(double), h, b.npts * sizeof(double),
+                            b.npts * sizeof(double), 24, cudaMemcpyHostToDevice, e->stream));
   AMSS_CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -231,15 +544,15 @@ extern "C" int amss_engine_set_state(amss_engine* e, int block, const double* h)
 extern "C" int amss_engine_get_state(amss_engine* e, int block, double* h) {
   if (int rc = check_block(e, block)) return rc;
   EBlock& b = e->blocks[block];
-  AMSS_CK(cudaMemcpy2DAsync(h, b.npts * sizeof(double), b.u0, b.fs * sizeof(double), b.npts * sizeof(double), 24,
-                            cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaMemcpy2DAsync(h, b.npts * sizeof(double), cur_state(e, b), b.fs * sizeof(double),
+                            b.npts * sizeof(double), 24, cudaMemcpyDeviceToHost, e->stream));
   AMSS_CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
 
 extern "C" int amss_engine_state_device(amss_engine* e, int block, double** dptr, long long* fs) {
   if (int rc = check_block(e, block)) return rc;
-  *dptr = e->blocks[block].u0;
+  *dptr = cur_state(e, e->blocks[block]);
   *fs = e->blocks[block].fs;
   return 0;
 }
@@ -247,12 +560,23 @@ extern "C" int amss_engine_state_device(amss_engine* e, int block, double** dptr
 extern "C" int amss_engine_enforce(amss_engine* e) {
   if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
   for (auto& b : e->blocks) {
-    AMSS_CK(launch_enforce(b.npts, b.fs, b.u0 + F_GXX * b.fs, b.u0 + F_AXX * b.fs, e->stream));
+    double* u = cur_state(e, b);
+    AMSS_CK(launch_enforce(b.npts, b.fs, u + F_GXX * b.fs, u + F_AXX * b.fs, e->stream));
     e->launches++;
   }
   return 0;
 }
 
+static int sync_level(amss_engine* e, ELevel& L, int which) {
+  if (L.sync.ntiles == 0) return 0;
+  AMSS_CK(launch_amr_sync(e->dblocks, L.sync.boxes, L.sync.tiles, L.sync.ntiles, which, e->prm.precision == 1,
+                          e->dstatus, e->stream));
+  e->launches++;
+  return 0;
+}
+
+// One RK4 step of every block of a level (bssn_class::Step, bssn_class.C:2981-3915):
+// four fused substep launches, a ghost sync after each, the ring rotation.
 static int step_level_impl(amss_engine* e, int level, double dt) {
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_step_level: no such level");
@@ -264,16 +588,80 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
   rk.chitiny = e->prm.chitiny;
   const bool mixed = e->prm.precision == 1;
   const int grid = std::min(L.ntiles, e->sm_count * 8);
+  // enforce_ga on U0 in place (bssn_class.C:3052); the stage outputs of
+  // substeps 0-2 are enforced as they are written, which equals the
+  // reference's in-place enforce_ga at the start of substeps 1-3 (:3416)
+  AMSS_CK(launch_amr_enforce(e->dblocks, L.dti_tiles, L.nti, e->stream));
+  e->launches++;
+  const bool split = e->prm.kernel == 0;
+  const int dgrid = std::min(L.nditems, e->sm_count * 16);
   for (int sub = 0; sub < 4; ++sub) {
     cudaError_t err;
+    const int enf = sub < 3 ? 1 : 0;
+    if (split) {
+      const cudaError_t ed = mixed ? launch_deriv<float, float>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream)
+                                   : launch_deriv<double, double>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream);
+      AMSS_CK(ed);
+      e->launches++;
+    }
+#define AMSS_SUB(T, SY, SP) \
+    launch_substep<T, T, SY, SP>(L.dtable, L.dtiles, L.ntiles, sub, rk, enf, e->dstatus, grid, e->stream, e->D, L.dfs)
     if (mixed)
-      err = L.symm ? launch_substep<float, float, true>(L.dtable, L.dtiles, L.ntiles, sub, rk, 1, e->dstatus, grid, e->stream)
-                   : launch_substep<float, float, false>(L.dtable, L.dtiles, L.ntiles, sub, rk, 1, e->dstatus, grid, e->stream);
+      err = split ? (L.symm ? AMSS_SUB(float, true, true) : AMSS_SUB(float, false, true))
+                  : (L.symm ? AMSS_SUB(float, true, false) : AMSS_SUB(float, false, false));
     else
-      err = L.symm ? launch_substep<double, double, true>(L.dtable, L.dtiles, L.ntiles, sub, rk, 1, e->dstatus, grid, e->stream)
-                   : launch_substep<double, double, false>(L.dtable, L.dtiles, L.ntiles, sub, rk, 1, e->dstatus, grid, e->stream);
+      err = split ? (L.symm ? AMSS_SUB(double, true, true) : AMSS_SUB(double, false, true))
+                  : (L.symm ? AMSS_SUB(double, true, false) : AMSS_SUB(double, false, false));
+#undef AMSS_SUB
     AMSS_CK(err);
     e->launches++;
+    if (sub < 3) {
+      if (int rc = sync_level(e, L, sub == 1 ? BUF_STAGE_B : BUF_STAGE_A)) return rc;
+    }
+  }
+  AMSS_CK(launch_amr_rotate(e->dlvl + 2 * level, e->stream));
+  e->launches++;
+  L.cur = (L.cur + 1) % 3;
+  L.steps++;
+  return sync_level(e, L, BUF_STATE);
+}
+
+// bssn_class::RestrictProlong (bssn_class.C:5724-5903) for level l > 0.
+static int restrict_prolong(amss_engine* e, int l, bool same_time) {
+  ELevel& F = e->levels[l];
+  ELevel& C = e->levels[l - 1];
+  if (!same_time) {
+    AMSS_CK(launch_amr_timeinterp(e->dblocks, C.dti_tiles, C.nti, e->stream));
+    e->launches++;
+  }
+  const int to_temp = same_time ? 0 : 1;
+  if (F.restrict_.ntiles) {
+    AMSS_CK(launch_amr_restrict(e->dblocks, F.restrict_.boxes, F.restrict_.tiles, F.restrict_.ntiles, to_temp,
+                                e->dstatus, e->stream));
+    e->launches++;
+  }
+  if (int rc = sync_level(e, C, same_time ? BUF_STATE : BUF_TEMP)) return rc;
+  if (F.prolong.ntiles) {
+    AMSS_CK(launch_amr_prolong(e->dblocks, F.prolong.boxes, F.prolong.tiles, F.prolong.ntiles, to_temp,
+                               e->dstatus, e->stream));
+    e->launches++;
+  }
+  return sync_level(e, F, BUF_STATE);
+}
+
+// bssn_class::RecursiveStep (bssn_class.C:2323-2414), PSTR 0, RPS 1, trfls 0:
+// level 0 takes one step, every finer level two per parent step.
+static int recursive_step(amss_engine* e, int l, double dt0) {
+  const int nlev = (int)e->levels.size();
+  const int iters = l == 0 ? 1 : 2;
+  const double dt = dt0 / std::ldexp(1.0, l);
+  for (int i = 0; i < iters; ++i) {
+    const bool yn = i == iters - 1;
+    if (int rc = step_level_impl(e, l, dt)) return rc;
+    if (l < nlev - 1)
+      if (int rc = recursive_step(e, l + 1, dt0)) return rc;
+    if (l > 0)
+      if (int rc = restrict_prolong(e, l, yn)) return rc;
   }
   return 0;
 }
@@ -283,26 +671,49 @@ extern "C" int amss_engine_step_level(amss_engine* e, int level, double dt) {
   return step_level_impl(e, level, dt);
 }
 
-extern "C" int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int replays) {
+extern "C" int amss_engine_coarse_step(amss_engine* e, double dt0) {
   if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  return recursive_step(e, 0, dt0);
+}
+
+// Capture `nsteps` of either a single-level step (level >= 0) or a coarse
+// Berger-Oliger step (level < 0) once as a graph and replay it.
+static int run_graph(amss_engine* e, int level, double dt, int nsteps, int replays) {
   cudaGraph_t g;
   cudaGraphExec_t ge;
-  AMSS_CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  std::vector<int> cur0;
+  std::vector<long long> steps0;
+  for (auto& kv : e->levels) { cur0.push_back(kv.second.cur); steps0.push_back(kv.second.steps); }
   const long long before = e->launches;
-  for (int s = 0; s < nsteps; ++s) {
-    const int rc = step_level_impl(e, level, dt);
-    if (rc) {
-      cudaStreamEndCapture(e->stream, &g);
-      return rc;
-    }
-  }
-  AMSS_CK(cudaStreamEndCapture(e->stream, &g));
+  AMSS_CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  for (int s = 0; s < nsteps && rc == 0; ++s) rc = level >= 0 ? step_level_impl(e, level, dt) : recursive_step(e, 0, dt);
+  cudaError_t ec = cudaStreamEndCapture(e->stream, &g);
+  if (rc) return rc;
+  AMSS_CK(ec);
   const long long per_replay = e->launches - before;
+  // capture issued nothing yet: undo the host mirrors and re-advance them per replay
+  std::vector<int> dcur;
+  std::vector<long long> dsteps;
+  size_t q = 0;
+  for (auto& kv : e->levels) {
+    dcur.push_back(((kv.second.cur - cur0[q]) % 3 + 3) % 3);
+    dsteps.push_back(kv.second.steps - steps0[q]);
+    kv.second.cur = cur0[q];
+    kv.second.steps = steps0[q];
+    ++q;
+  }
   e->launches = before;
   AMSS_CK(cudaGraphInstantiate(&ge, g, 0));
   for (int r = 0; r < replays; ++r) {
     AMSS_CK(cudaGraphLaunch(ge, e->stream));
     e->launches += per_replay;
+    q = 0;
+    for (auto& kv : e->levels) {
+      kv.second.cur = (kv.second.cur + dcur[q]) % 3;
+      kv.second.steps += dsteps[q];
+      ++q;
+    }
   }
   AMSS_CK(cudaStreamSynchronize(e->stream));
   cudaGraphExecDestroy(ge);
@@ -310,13 +721,34 @@ extern "C" int amss_engine_run_graph(amss_engine* e, int level, double dt, int n
   return 0;
 }
 
+extern "C" int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int replays) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (level < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_run_graph: level must be >= 0");
+  return run_graph(e, level, dt, nsteps, replays);
+}
+
+extern "C" int amss_engine_run_coarse_graph(amss_engine* e, double dt0, int nsteps, int replays) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  return run_graph(e, -1, dt0, nsteps, replays);
+}
+
 extern "C" int amss_engine_sync(amss_engine* e) {
   if (!e) return AMSS_ERR_ARG;
   AMSS_CK(cudaStreamSynchronize(e->stream));
   unsigned st = 0;
   AMSS_CK(cudaMemcpy(&st, e->dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (st & ST_BAD_ARG) return amss_fail(AMSS_ERR_STATE, "a kernel met a box outside its block (engine tables)");
   return ((st & ST_NAN) || ((st & ST_PINF) && (st & ST_NINF))) ? 1 : 0;
 }
 
 extern "C" void* amss_engine_stream(amss_engine* e) { return e ? (void*)e->stream : nullptr; }
 extern "C" long long amss_engine_launch_count(amss_engine* e) { return e ? e->launches : 0; }
+
+extern "C" long long amss_engine_level_points(amss_engine* e, int level) {
+  if (!e) return -1;
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return 0;
+  long long n = 0;
+  for (int b : it->second.blocks) n += e->blocks[b].npts;
+  return n;
+}

@@ -2,6 +2,6 @@
 #include "substep_impl.cuh"
 
 namespace amss {
-template cudaError_t launch_rhs_dropin<true>(int, cudaStream_t, BlockView, Coef<double>, const double*, double*,
+template cudaError_t launch_rhs_dropin<true>(int, cudaStream_t, BlockView, Coefs<double>, const double*, double*,
                                             RhsAux, unsigned*);
 }  // namespace amss

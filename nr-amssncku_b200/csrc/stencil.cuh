@@ -7,6 +7,8 @@
 // and kodiss.f90:190-207, so that FP64 results agree with the reference to
 // round-off.
 #pragma once
+#include <type_traits>
+
 #include "amss_common.cuh"
 
 namespace amss {
@@ -25,30 +27,58 @@ struct Coef {
   T ko;              // eps/64
 };
 
+// chi and alpha carry O(1) backgrounds: an FP32 copy of them costs ~6e-8 * |f|
+// absolute, which a second derivative turns into a relative RHS error of
+// ~6e-8 (L/dx)^2.  In the mixed form they therefore keep FP64 stage storage
+// ("side" arrays) and FP64 stencil arithmetic; every other field is FP32.
+template <int F>
+__host__ __device__ constexpr bool wide_field() { return F == F_CHI || F == F_LAP; }
+__host__ __device__ constexpr int side_slot(int F) { return F == F_CHI ? 0 : 1; }
+
+// Coefficients in the arithmetic type and in FP64 (for the wide fields).
+template <typename T>
+struct Coefs {
+  Coef<T> t;
+  Coef<double> d;
+};
+template <typename A, typename T>
+__device__ __forceinline__ const Coef<A>& pick(const Coefs<T>& C) {
+  if constexpr (std::is_same_v<A, T>) return C.t;
+  else return C.d;
+}
+
 // Point accessor.  With SYMM == false, offsets are applied directly: callers
 // only step outside [0, ex) where the reference reads its symmetry pad.  With
 // SYMM == true every access mirrors negative indices cell-centred,
 // f(-m) = f(m-1) * parity (fmisc.f90:877-901), which also covers that pad.
 template <typename SI, bool SYMM>
 struct Pt {
+  static constexpr bool kPre = false;
+  using elem = SI;
   const SI* __restrict__ base;  // field 0 of the block
+  const double* __restrict__ side;  // FP64 chi, alpha when SI is float (else unused)
   long long fs;                 // field stride
   long long p;                  // linear index of the point
   long long sy, sz;             // strides of j and k
   int i, j, k;                  // 0-based indices
   int ex0, ex1, ex2;
 
+  template <int F>
+  __device__ __forceinline__ auto ld(long long idx) const {
+    if constexpr (sizeof(SI) == 4 && wide_field<F>()) return __ldg(side + side_slot(F) * fs + idx);
+    else return __ldg(base + F * fs + idx);
+  }
   template <typename T, int F>
   __device__ __forceinline__ T v(int di, int dj, int dk) const {
     if constexpr (!SYMM) {
-      return (T)__ldg(base + F * fs + p + di + dj * sy + dk * sz);
+      return (T)ld<F>(p + di + dj * sy + dk * sz);
     } else {
       int ii = i + di, jj = j + dj, kk = k + dk;
       bool neg = false;
       if (ii < 0) { ii = -ii - 1; neg ^= (soa_sign(F, 0) < 0); }
       if (jj < 0) { jj = -jj - 1; neg ^= (soa_sign(F, 1) < 0); }
       if (kk < 0) { kk = -kk - 1; neg ^= (soa_sign(F, 2) < 0); }
-      T x = (T)__ldg(base + F * fs + ii + jj * sy + kk * sz);
+      T x = (T)ld<F>(ii + jj * sy + kk * sz);
       return neg ? -x : x;
     }
   }
@@ -60,9 +90,39 @@ struct Pt {
     if (ii < 0) { ii = -ii - 1; neg ^= (soa_sign(F, 0) < 0); }
     if (jj < 0) { jj = -jj - 1; neg ^= (soa_sign(F, 1) < 0); }
     if (kk < 0) { kk = -kk - 1; neg ^= (soa_sign(F, 2) < 0); }
-    T x = (T)__ldg(base + F * fs + ii + jj * sy + kk * sz);
+    T x = (T)ld<F>(ii + jj * sy + kk * sz);
     return neg ? -x : x;
   }
+};
+
+// ---- precomputed stencil terms (split form) ----------------------------------
+// The stencil pass (deriv.cuh) stores, per point and field, what the RHS needs
+// of that field's neighbourhood: gradient (3), Hessian (6: xx xy xz yy yz zz),
+// the summed upwinded advection and the summed KO line sums -- 11 values for
+// the shift, chi, the metric and the lapse, 5 for trK and Gamma^i (gradient,
+// advection, KO), 2 for A~ij and B^i (advection, KO): 159 slots in all.
+__host__ __device__ constexpr int dslots(int F) {
+  return (F == F_BETAX || F == F_BETAY || F == F_BETAZ || F == F_CHI || F == F_LAP || (F >= F_GXX && F <= F_GZZ))
+             ? 11
+             : ((F == F_TRK || F == F_GAMX || F == F_GAMY || F == F_GAMZ) ? 5 : 2);
+}
+__host__ __device__ constexpr int doff(int F) {
+  int o = 0;
+  for (int f = 0; f < F; ++f) o += dslots(f);
+  return o;
+}
+constexpr int D_SLOTS = 159;
+static_assert(doff(24) == D_SLOTS, "D slot layout");
+
+// Accessor of the pointwise pass: centre values from the stage input (Pt),
+// stencil terms from the D array written by the stencil pass.
+template <typename SI, bool SYMM, typename DT>
+struct DPt : Pt<SI, SYMM> {
+  static constexpr bool kPre = true;
+  const DT* __restrict__ d;   // slot 0 of this point's block (add slot * dfs + p)
+  long long dfs;              // slot stride
+  template <typename T>
+  __device__ __forceinline__ T dv(int slot) const { return (T)__ldg(d + slot * dfs + this->p); }
 };
 
 template <int D>
@@ -88,7 +148,7 @@ __device__ __forceinline__ T d1o2(const P& q, const Coef<T>& C) {
 // Gradient of field F with the reference's joint order gate: ord 2 = 4th order,
 // 1 = 2nd order, 0 = derivative is zero (diff_new.f90:1084-1096).
 template <typename T, int F, typename P>
-__device__ __forceinline__ void grad(const P& q, const Coef<T>& C, int ord, T& fx, T& fy, T& fz) {
+__device__ __forceinline__ void grad_a(const P& q, const Coef<T>& C, int ord, T& fx, T& fy, T& fz) {
   if (ord == 2) {
     fx = d1o4<T, F, 0>(q, C); fy = d1o4<T, F, 1>(q, C); fz = d1o4<T, F, 2>(q, C);
   } else if (ord == 1) {
@@ -96,6 +156,17 @@ __device__ __forceinline__ void grad(const P& q, const Coef<T>& C, int ord, T& f
   } else {
     fx = T(0); fy = T(0); fz = T(0);
   }
+}
+template <typename T, int F, typename P>
+__device__ __forceinline__ void grad(const P& q, const Coefs<T>& C, int ord, T& fx, T& fy, T& fz) {
+  if constexpr (P::kPre) {
+    fx = q.template dv<T>(doff(F) + 0); fy = q.template dv<T>(doff(F) + 1); fz = q.template dv<T>(doff(F) + 2);
+    return;
+  }
+  using A = std::conditional_t<wide_field<F>(), double, T>;
+  A ax, ay, az;
+  grad_a<A, F>(q, pick<A>(C), ord, ax, ay, az);
+  fx = (T)ax; fy = (T)ay; fz = (T)az;
 }
 
 // ---- second derivatives (fdderivs) ------------------------------------------
@@ -140,8 +211,8 @@ __device__ __forceinline__ T dmo2(const P& q, T coef) {
 
 // Hessian of F: fxx fxy fxz fyy fyz fzz (fdderivs output order).
 template <typename T, int F, typename P>
-__device__ __forceinline__ void hess(const P& q, const Coef<T>& C, int ord, T& fxx, T& fxy, T& fxz, T& fyy,
-                                     T& fyz, T& fzz) {
+__device__ __forceinline__ void hess_a(const P& q, const Coef<T>& C, int ord, T& fxx, T& fxy, T& fxz, T& fyy,
+                                       T& fyz, T& fzz) {
   if (ord == 2) {
     fxx = d2o4<T, F, 0>(q, C); fyy = d2o4<T, F, 1>(q, C); fzz = d2o4<T, F, 2>(q, C);
     fxy = dmo4<T, F, 0, 1>(q, C.Fxy); fxz = dmo4<T, F, 0, 2>(q, C.Fxz); fyz = dmo4<T, F, 1, 2>(q, C.Fyz);
@@ -152,34 +223,64 @@ __device__ __forceinline__ void hess(const P& q, const Coef<T>& C, int ord, T& f
     fxx = fxy = fxz = fyy = fyz = fzz = T(0);
   }
 }
+template <typename T, int F, typename P>
+__device__ __forceinline__ void hess(const P& q, const Coefs<T>& C, int ord, T& fxx, T& fxy, T& fxz, T& fyy,
+                                     T& fyz, T& fzz) {
+  if constexpr (P::kPre) {
+    const int o = doff(F) + 3;
+    fxx = q.template dv<T>(o); fxy = q.template dv<T>(o + 1); fxz = q.template dv<T>(o + 2);
+    fyy = q.template dv<T>(o + 3); fyz = q.template dv<T>(o + 4); fzz = q.template dv<T>(o + 5);
+    return;
+  }
+  using A = std::conditional_t<wide_field<F>(), double, T>;
+  A a[6];
+  hess_a<A, F>(q, pick<A>(C), ord, a[0], a[1], a[2], a[3], a[4], a[5]);
+  fxx = (T)a[0]; fxy = (T)a[1]; fxz = (T)a[2]; fyy = (T)a[3]; fyz = (T)a[4]; fzz = (T)a[5];
+}
 
 // ---- upwinded advection (lopsided), one direction ---------------------------
 // Returns r + beta * D^upwind f along D following lopsidediff.f90:321-481;
 // `add1` is 1 when the advected array is the full metric g = d + 1.
 // lo/hi are the reference's imin/imax in 0-based form.
 template <typename T, int F, int D, typename P>
-__device__ __forceinline__ T lop_dir(const P& q, const Coef<T>& C, T r, T b, int idx, int lo, int hi, T add1) {
-  const T F3 = T(3), F10 = T(10), F18 = T(18), F6 = T(6), EIT = T(8);
-  auto f = [&](int o) -> T {
-    return q.template vpad<T, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)) + add1;
+__device__ __forceinline__ T lop_dir(const P& q, const Coefs<T>& CC, T r, T b, int idx, int lo, int hi, T add1) {
+  using A = std::conditional_t<wide_field<F>(), double, T>;
+  const Coef<A>& C = pick<A>(CC);
+  const A F3 = A(3), F10 = A(10), F18 = A(18), F6 = A(6), EIT = A(8);
+  auto f = [&](int o) -> A {
+    return q.template vpad<A, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)) + A(add1);
   };
-  const T bd = b * C.d12[D];
-  if (b > T(0)) {
-    if (idx + 3 <= hi)
-      r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
-    else if (idx + 2 <= hi)
-      r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
-    else if (idx + 1 <= hi)
-      r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
-  } else if (b < T(0)) {
-    if (idx - 3 >= lo)
-      r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
-    else if (idx - 2 >= lo)
-      r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
-    else if (idx - 1 >= lo)
-      r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+  const A bd = A(b) * C.d12[D];
+  if constexpr (std::is_same_v<A, T>) {
+    if (b > T(0)) {
+      if (idx + 3 <= hi)
+        r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+      else if (idx + 2 <= hi)
+        r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+      else if (idx + 1 <= hi)
+        r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+    } else if (b < T(0)) {
+      if (idx - 3 >= lo)
+        r = r - bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+      else if (idx - 2 >= lo)
+        r = r + bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+      else if (idx - 1 >= lo)
+        r = r + bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+    }
+    return r;
+  } else {
+    A d = A(0);
+    if (b > T(0)) {
+      if (idx + 3 <= hi) d = bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+      else if (idx + 2 <= hi) d = bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+      else if (idx + 1 <= hi) d = -bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+    } else if (b < T(0)) {
+      if (idx - 3 >= lo) d = -bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+      else if (idx - 2 >= lo) d = bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+      else if (idx - 1 >= lo) d = bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+    }
+    return r + (T)d;
   }
-  return r;
 }
 
 // ---- Kreiss-Oliger, combined directions (kodiss.f90:190-207) ----------------

@@ -2,7 +2,7 @@
 // Instantiated in one translation unit per (precision, symmetry) pair so the
 // large kernels compile in parallel.
 #pragma once
-#include "bssn_step.cuh"
+#include "deriv.cuh"
 
 namespace amss {
 
@@ -15,9 +15,11 @@ __device__ __forceinline__ void point_ijk(long long p, const int* ex, int& i, in
 }
 
 template <typename SI, bool SYMM>
-__device__ __forceinline__ Pt<SI, SYMM> make_pt(const SI* base, const BlockView& b, long long p) {
+__device__ __forceinline__ Pt<SI, SYMM> make_pt(const SI* base, const BlockView& b, long long p,
+                                               const double* side = nullptr) {
   Pt<SI, SYMM> q;
   q.base = base;
+  q.side = side;
   q.fs = b.fs;
   q.p = p;
   q.sy = b.ex[0];
@@ -31,19 +33,26 @@ __device__ __forceinline__ Pt<SI, SYMM> make_pt(const SI* base, const BlockView&
 
 // Fused RK4 substep over a tile list of one level.  Substep `sub` reads
 // (sub0: u0, sub1: A, sub2: B, sub3: A) and writes (A, B, A, unew).
-template <typename T, typename SI, typename SO, bool SYMM>
+// SPLIT: the stencil terms come from the D array the stencil pass (k_deriv)
+// wrote for this substep; otherwise every stencil is evaluated here.
+template <typename T, typename SI, typename SO, bool SYMM, bool SPLIT>
 __global__ void __launch_bounds__(128) k_substep(const StepBlock<T>* __restrict__ blocks, const int2* __restrict__ tiles,
-                                                 int ntiles, int sub, RKConst rk, int enforce, unsigned* status) {
+                                                 int ntiles, int sub, RKConst rk, int enforce, unsigned* status,
+                                                 const T* __restrict__ D, long long dfs) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
     const StepBlock<T>& B = blocks[tile.x];
     const long long p = (long long)tile.y + threadIdx.x;
     if (p >= B.npts) continue;
-    const SI* in = sub == 0 ? (const SI*)B.u0 : (const SI*)B.stage[sub == 2 ? 1 : 0];
-    SO* out = sub == 3 ? (SO*)B.unew : (SO*)B.stage[sub == 1 ? 1 : 0];
-    auto q = make_pt<SI, SYMM>(in, B.b, p);
+    const int cur = B.lvl[0];
+    double* u0 = B.tl[cur];
+    const SI* in = sub == 0 ? (const SI*)u0 : (const SI*)B.stage[sub == 2 ? 1 : 0];
+    SO* out = sub == 3 ? (SO*)B.tl[(cur + 1) % 3] : (SO*)B.stage[sub == 1 ? 1 : 0];
+    const double* in_side = sub == 0 ? nullptr : B.side[sub == 2 ? 1 : 0];
+    auto q = make_pt<SI, SYMM>(in, B.b, p, in_side);
     EpiRK<T, SO> epi;
-    epi.u0 = B.u0;
+    epi.out_side = sub == 3 ? nullptr : B.side[sub == 1 ? 1 : 0];
+    epi.u0 = u0;
     epi.K = B.K;
     epi.out = out;
     epi.fs = B.b.fs;
@@ -60,7 +69,15 @@ __global__ void __launch_bounds__(128) k_substep(const StepBlock<T>* __restrict_
     if (!on_face) {
       const PointGates G = point_gates(B.b, q.i, q.j, q.k);
       RhsAux aux{};
-      st = bssn_rhs_point<T, SI, SYMM, false>(q, B.C, G, aux, epi);
+      if constexpr (SPLIT) {
+        DPt<SI, SYMM, T> qd;
+        static_cast<Pt<SI, SYMM>&>(qd) = q;
+        qd.d = D + B.doff;
+        qd.dfs = dfs;
+        st = bssn_rhs_point<T, SI, SYMM, false>(qd, B.C, G, aux, epi);
+      } else {
+        st = bssn_rhs_point<T, SI, SYMM, false>(q, B.C, G, aux, epi);
+      }
     } else {
       // NaN check of the input, as the full RHS would do it
       T chk[21];
@@ -109,18 +126,39 @@ __global__ void __launch_bounds__(128) k_substep(const StepBlock<T>* __restrict_
   }
 }
 
-template <typename T, typename SS, bool SYMM>
+template <typename T, typename SS, bool SYMM, bool SPLIT>
 cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, int sub, RKConst rk, int enforce,
-                           unsigned* status, int grid, cudaStream_t s) {
+                           unsigned* status, int grid, cudaStream_t s, const void* D, long long dfs) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
-  if (sub == 0) k_substep<T, double, SS, SYMM><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status);
-  else if (sub == 3) k_substep<T, SS, double, SYMM><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status);
-  else k_substep<T, SS, SS, SYMM><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status);
+  const T* d = (const T*)D;
+  if (sub == 0)
+    k_substep<T, double, SS, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  else if (sub == 3)
+    k_substep<T, SS, double, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  else
+    k_substep<T, SS, SS, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
   return cudaGetLastError();
 }
+
+// Stencil pass launcher: substep 0 reads the FP64 state, 1-3 the stages.
+template <typename T, typename SS>
+cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
+                         int grid, cudaStream_t s) {
+  const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
+  const size_t smem = 7 * DPLANE * sizeof(double);
+  if (sub == 0) {
+    cudaFuncSetAttribute(k_deriv<T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_deriv<T, double><<<grid, DTX * DTY, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  } else {
+    cudaFuncSetAttribute(k_deriv<T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_deriv<T, SS><<<grid, DTX * DTY, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  }
+  return cudaGetLastError();
+}
+
 // Drop-in RHS: all points of one block, RHS plus the diagnostic outputs.
 template <bool SYMM>
-__global__ void __launch_bounds__(128) k_rhs_dropin(BlockView b, Coef<double> C, const double* __restrict__ u,
+__global__ void __launch_bounds__(128) k_rhs_dropin(BlockView b, Coefs<double> C, const double* __restrict__ u,
                                                     double* __restrict__ rhs, RhsAux aux, unsigned* status) {
   const long long n = (long long)b.ex[0] * b.ex[1] * b.ex[2];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
@@ -133,7 +171,7 @@ __global__ void __launch_bounds__(128) k_rhs_dropin(BlockView b, Coef<double> C,
 }
 
 template <bool SYMM>
-cudaError_t launch_rhs_dropin(int grid, cudaStream_t s, BlockView b, Coef<double> C, const double* u, double* rhs,
+cudaError_t launch_rhs_dropin(int grid, cudaStream_t s, BlockView b, Coefs<double> C, const double* u, double* rhs,
                               RhsAux aux, unsigned* status) {
   k_rhs_dropin<SYMM><<<grid, 128, 0, s>>>(b, C, u, rhs, aux, status);
   return cudaGetLastError();

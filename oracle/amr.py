@@ -1,0 +1,226 @@
+"""CPU oracle of a Berger-Oliger evolution over a block hierarchy (test infrastructure only).
+
+Follows, block by block and in the reference's order:
+  bssn_class::RecursiveStep   bssn_class.C:2323-2414 (PSTR 0, RPS 1, trfls 0)
+  bssn_class::Step            bssn_class.C:2981-3915 (per block substep via
+                              oracle_bssn_substep, then Parallel::Sync)
+  bssn_class::RestrictProlong bssn_class.C:5724-5903
+  Parallel::prepare_inter_time_level Parallel.C:4329-4441 (average / average2)
+with restrict3 / prolong3 from amr_oracle.c.  The hierarchy (patches, buffer
+cells, blocks, ghost cells) is the plain description of
+amss_b200.hierarchy.Hierarchy.  Parity unpinned (see oracle_common.h).
+"""
+import ctypes
+
+import numpy as np
+
+import oracle as O
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_I3 = ctypes.c_int * 3
+
+
+def _p(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _ptrs(arr):
+    return (_DP * 24)(*[_p(arr[f]) for f in range(24)])
+
+
+def _isect(alo, ahi, blo, bhi):
+    lo = tuple(max(a, b) for a, b in zip(alo, blo))
+    hi = tuple(min(a, b) for a, b in zip(ahi, bhi))
+    return (lo, hi) if all(l < h for l, h in zip(lo, hi)) else None
+
+
+class OracleHierarchy:
+    def __init__(self, H, eps=0.1, chitiny=1e-5 - 1.0, symmetry=0):
+        self.H = H
+        self.eps = eps
+        self.chitiny = chitiny
+        self.symmetry = symmetry
+        lib = O.lib()
+        lib.oracle_bssn_substep.restype = ctypes.c_int
+        self.blk = []
+        for b in H.blocks:
+            shape = (24, b.ex[2], b.ex[1], b.ex[0])
+            X, Y, Z = H.coords(b)
+            p = H.levels[b.level][b.patch]
+            self.blk.append(dict(
+                U=[np.zeros(shape) for _ in range(3)], K=np.zeros(shape), A=np.zeros(shape), B=np.zeros(shape),
+                X=X, Y=Y, Z=Z, pbbox=np.array(H.patch_bbox(p)), ex=(ctypes.c_int * 3)(*b.ex)))
+        self.cur = [0] * len(H.levels)
+        self.steps = [0] * len(H.levels)
+
+    # state access ------------------------------------------------------------
+    def state(self, bi):
+        b = self.H.blocks[bi]
+        return self.blk[bi]["U"][self.cur[b.level]]
+
+    def set_state(self, bi, st):
+        self.state(bi)[...] = st
+
+    def _arr(self, bi, which):
+        d = self.blk[bi]
+        if which == "state":
+            return self.state(bi)
+        return d[which]
+
+    @staticmethod
+    def _view(b, arr, lo, hi):
+        sl = tuple(slice(lo[d] - b.org[d], hi[d] - b.org[d]) for d in (2, 1, 0))
+        return arr[(slice(None),) + sl]
+
+    # Parallel::Sync ------------------------------------------------------------
+    def sync(self, level, which):
+        ids = [i for p in self.H.levels[level] for i in p.blocks]
+        for d in ids:
+            bd = self.H.blocks[d]
+            alo, ahi = bd.org, tuple(bd.org[k] + bd.ex[k] for k in range(3))
+            for s in ids:
+                if s == d:
+                    continue
+                bs = self.H.blocks[s]
+                r = _isect(alo, ahi, bs.own_lo, bs.own_hi)
+                if r:
+                    self._view(bd, self._arr(d, which), *r)[...] = self._view(bs, self._arr(s, which), *r)
+
+    # bssn_class::Step ----------------------------------------------------------
+    def level_step(self, level, dt):
+        lib = O.lib()
+        ids = [i for p in self.H.levels[level] for i in p.blocks]
+        c = self.cur[level]
+        err = 0
+        for sub in range(4):
+            for bi in ids:
+                d = self.blk[bi]
+                u0 = d["U"][c]
+                src = {0: u0, 1: d["A"], 2: d["B"], 3: d["A"]}[sub]
+                out = {0: d["A"], 1: d["B"], 2: d["A"], 3: d["U"][(c + 1) % 3]}[sub]
+                err |= lib.oracle_bssn_substep(d["ex"], _p(d["X"]), _p(d["Y"]), _p(d["Z"]), _p(d["pbbox"]),
+                                               _ptrs(u0), _ptrs(src), _ptrs(out), _ptrs(d["K"]), ctypes.c_int(sub),
+                                               ctypes.c_double(dt), ctypes.c_double(self.eps),
+                                               ctypes.c_double(self.chitiny), ctypes.c_int(self.symmetry),
+                                               ctypes.c_int(level))
+            if sub < 3:
+                self.sync(level, "A" if sub != 1 else "B")
+        self.cur[level] = (c + 1) % 3
+        self.steps[level] += 1
+        self.sync(level, "state")
+        return err
+
+    # bssn_class::RestrictProlong ------------------------------------------------
+    def restrict_prolong(self, level, same_time):
+        lib = O.lib()
+        H = self.H
+        cl = level - 1
+        cids = [i for p in H.levels[cl] for i in p.blocks]
+        if not same_time:
+            c = self.cur[cl]
+            for bi in cids:
+                d = self.blk[bi]
+                f1, f2, f3 = d["U"][c], d["U"][(c + 2) % 3], d["U"][(c + 1) % 3]
+                if self.steps[cl] >= 2:
+                    lib.oracle_average2(ctypes.c_long(f1.size), _p(f1), _p(f2), _p(f3), _p(d["K"]))
+                else:
+                    d["K"][...] = 0.5 * (f1 + f2)
+        ctarget = "state" if same_time else "K"
+        for p in H.levels[level]:
+            cphys_lo = tuple(v // 2 for v in p.lo)
+            cphys_hi = tuple(v // 2 for v in p.hi)
+            for cb in cids:
+                bc = H.blocks[cb]
+                r = _isect(cphys_lo, cphys_hi, bc.org, tuple(bc.org[k] + bc.ex[k] for k in range(3)))
+                if not r:
+                    continue
+                for fb in p.blocks:
+                    bf = H.blocks[fb]
+                    rr = _isect(r[0], r[1], tuple(v // 2 for v in bf.own_lo), tuple(v // 2 for v in bf.own_hi))
+                    if not rr:
+                        continue
+                    carr = self._arr(cb, ctarget)
+                    farr = self.state(fb)
+                    for f in range(24):
+                        lib.oracle_restrict3_box(_I3(*bc.ex), _I3(*bc.org), _p(carr[f]), _I3(*bf.ex), _I3(*bf.org),
+                                                 _p(farr[f]), _I3(*rr[0]), _I3(*rr[1]))
+        self.sync(cl, ctarget)
+        for p in H.levels[level]:
+            elo, ehi = p.ext_lo, p.ext_hi
+            slabs = []
+            for d in range(3):
+                lo_a, hi_a = list(elo), list(ehi)
+                lo_b, hi_b = list(elo), list(ehi)
+                for q in range(d):
+                    lo_a[q] = lo_b[q] = p.lo[q]
+                    hi_a[q] = hi_b[q] = p.hi[q]
+                hi_a[d] = p.lo[d]
+                lo_b[d] = p.hi[d]
+                slabs += [(tuple(lo_a), tuple(hi_a)), (tuple(lo_b), tuple(hi_b))]
+            for fb in p.blocks:
+                bf = H.blocks[fb]
+                for slo, shi in slabs:
+                    r = _isect(slo, shi, bf.org, tuple(bf.org[k] + bf.ex[k] for k in range(3)))
+                    if not r:
+                        continue
+                    for cb in cids:
+                        bc = H.blocks[cb]
+                        rr = _isect(r[0], r[1], tuple(2 * v for v in bc.own_lo), tuple(2 * v for v in bc.own_hi))
+                        if not rr:
+                            continue
+                        carr = self._arr(cb, ctarget)
+                        farr = self.state(fb)
+                        for f in range(24):
+                            lib.oracle_prolong3_box(_I3(*bc.ex), _I3(*bc.org), _p(carr[f]), _I3(*bf.ex),
+                                                    _I3(*bf.org), _p(farr[f]), _I3(*rr[0]), _I3(*rr[1]))
+        self.sync(level, "state")
+
+    # bssn_class::RecursiveStep ---------------------------------------------------
+    def recursive_step(self, level, dt0):
+        iters = 1 if level == 0 else 2
+        dt = dt0 / 2 ** level
+        err = 0
+        for i in range(iters):
+            yn = i == iters - 1
+            err |= self.level_step(level, dt)
+            if level < len(self.H.levels) - 1:
+                err |= self.recursive_step(level + 1, dt0)
+            if level > 0:
+                self.restrict_prolong(level, yn)
+        return err
+
+    def coarse_step(self, dt0):
+        return self.recursive_step(0, dt0)
+
+
+def grid_noise(level, field, gi, gj, gk, seed):
+    """Uniform noise in [-1, 1) as a function of (seed, level, field, global
+    cell index) only, so every copy of a cell (owner, ghost, buffer) agrees.
+    splitmix64 finaliser over the packed key."""
+    key = (np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
+           ^ (np.uint64(level) << np.uint64(56)) ^ (np.uint64(field) << np.uint64(48))
+           ^ ((gk.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(32))
+           ^ ((gj.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(16))
+           ^ (gi.astype(np.uint64) & np.uint64(0xFFFF)))
+    z = key + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 / 2.0 ** 53) - 1.0
+
+
+def initial_state(H, masses, positions, noise=0.0, seed=1):
+    """Brill-Lindquist data on every block (get_lousto_nbhs), plus uniform noise
+    of amplitude `noise` that depends only on the global cell (grid_noise)."""
+    out = []
+    with np.errstate(over="ignore"):
+        for b in H.blocks:
+            X, Y, Z = H.coords(b)
+            st = O.brill_lindquist(X, Y, Z, masses, positions)
+            if noise > 0:
+                gk, gj, gi = np.meshgrid(np.arange(b.ex[2]) + b.org[2], np.arange(b.ex[1]) + b.org[1],
+                                         np.arange(b.ex[0]) + b.org[0], indexing="ij")
+                for f in range(24):
+                    st[f] += noise * grid_noise(b.level, f, gi, gj, gk, seed)
+            out.append(st)
+    return out

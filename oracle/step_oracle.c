@@ -443,3 +443,43 @@ int oracle_bssn_step_single(const int *ex, const double *X, const double *Y, con
     free(buf);
     return err;
 }
+
+/*
+ * One RK4 substep of one block, as bssn_class::Step runs it per block
+ * (bssn_class.C:3043-3158 for sub == 0, :3401-3525 for sub = 1..3):
+ * enforce_ga on the stage input (in place), compute_rhs_bssn, then per field
+ * sommerfeld_routbam (lev == 0), rungekutta4_rout, sommerfeld_rout precor=1
+ * (lev > 0), then lowerboundset on the stage output.
+ *   sub == 0: input u0, rhs -> K, output -> out
+ *   sub >= 1: input in,  rhs -> out (the reference's SynchList_cor), output -> out
+ * pbbox is the patch bbox (with buffer) that decides the outer faces.
+ * Returns the NaN flag of compute_rhs_bssn.
+ */
+int oracle_bssn_substep(const int *ex, const double *X, const double *Y, const double *Z, const double *pbbox,
+                        double **u0, double **in, double **out, double **K, int sub, double dT, double eps,
+                        double chitiny, int Symmetry, int lev)
+{
+    long n = npts3(ex);
+    double *buf = oalloc(n * (24 + 7 + 1));
+    double *scr[24], *cons[7];
+    for (int f = 0; f < 24; ++f) scr[f] = buf + n * f;
+    for (int c = 0; c < 7; ++c) cons[c] = buf + n * (24 + c);
+    double *zero = buf + n * 31;
+    double **src = sub == 0 ? u0 : in;
+    double **rtarget = sub == 0 ? K : out;
+    oracle_enforce_ga(ex, src[2], src[3], src[4], src[5], src[6], src[7], src[8], src[9], src[10], src[11], src[12],
+                      src[13]);
+    int err = rhs_call(ex, 0.0, X, Y, Z, src, rtarget, scr, zero, Symmetry, lev, eps, 1, cons);
+    for (int f = 0; f < 24; ++f) {
+        if (lev == 0)
+            oracle_sommerfeld_routbam(ex, X, Y, Z, pbbox[0], pbbox[1], pbbox[2], pbbox[3], pbbox[4], pbbox[5],
+                                      rtarget[f], src[f], oracle_bssn_propspeed(f), oracle_bssn_soa(f), Symmetry);
+        oracle_rungekutta4_rout(ex, dT, u0[f], out[f], K[f], sub);
+        if (lev > 0)
+            oracle_sommerfeld_rout(ex, X, Y, Z, pbbox[0], pbbox[1], pbbox[2], pbbox[3], pbbox[4], pbbox[5], u0[f],
+                                   out[f], Symmetry, 1);
+    }
+    oracle_lowerboundset(ex, out[0], chitiny);
+    free(buf);
+    return err;
+}

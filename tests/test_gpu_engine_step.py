@@ -2,10 +2,9 @@
 single-block level-0 step (enforce_ga, compute_rhs_bssn, sommerfeld_routbam,
 rungekutta4_rout, lowerboundset per substep, bssn_class.C:2981-3915).
 
-The engine applies enforce_ga to what a substep writes, so its state after a
-step is enforce_ga of the reference's; the comparison applies enforce_ga to
-the oracle's result.  FP64 bar 1e-12; mixed-precision bar 1e-6 (relative
-max-norm per field)."""
+The engine's state after a step equals the reference's (enforce_ga runs in
+place on U0 at the start of each step, as bssn_class.C:3052 does).  FP64 bar
+1e-12; mixed-precision bar 1e-6 (relative max-norm per field)."""
 import numpy as np
 import pytest
 
@@ -17,13 +16,12 @@ from helpers import generic_state, relerr
 pytestmark = pytest.mark.gpu
 
 
-def _run(precision, st0, X, bbox, dt, nsteps, eps=0.1):
+def _run(precision, st0, X, bbox, dt, nsteps, eps=0.1, kernel="split"):
     n = len(X)
-    e = amss_b200.Engine(precision=precision, eps=eps)
+    e = amss_b200.Engine(precision=precision, eps=eps, kernel=kernel)
     b = e.add_block(0, (n, n, n), bbox, bbox)
     e.commit()
     e.set_state(b, st0)
-    e.enforce()
     for _ in range(nsteps):
         e.step(0, dt)
     assert e.sync() == 0
@@ -36,12 +34,12 @@ def _oracle(st0, X, bbox, dt, nsteps, eps=0.1):
     st = st0.copy()
     for _ in range(nsteps):
         O.bssn_step_single(X, X, X, bbox, st, dt, eps=eps)
-    O.enforce_ga(st)
     return st
 
 
+@pytest.mark.parametrize("kernel", ["split", "fused"])
 @pytest.mark.parametrize("case", ["bl", "generic"])
-def test_fp64_step_matches_oracle(case):
+def test_fp64_step_matches_oracle(case, kernel):
     if case == "bl":
         X, st0, bbox, h = O.single_block_setup(24, -6.0, 6.0, 3, [1.0], [[0.1, 0.05, 0.02]], noise=1e-8)
     else:
@@ -51,16 +49,17 @@ def test_fp64_step_matches_oracle(case):
         st0 = generic_state(X, X, X, seed=12, amp=0.5)
     dt = 0.25 * h
     ref = _oracle(st0, X, bbox, dt, 3)
-    got = _run("fp64", st0, X, bbox, dt, 3)
+    got = _run("fp64", st0, X, bbox, dt, 3, kernel=kernel)
     errs = [relerr(got[f], ref[f]) for f in range(24)]
     assert max(errs) <= 1e-12, errs
 
 
-def test_mixed_step_error_bound():
+@pytest.mark.parametrize("kernel", ["split", "fused"])
+def test_mixed_step_error_bound(kernel):
     X, st0, bbox, h = O.single_block_setup(24, -6.0, 6.0, 3, [1.0], [[0.1, 0.05, 0.02]], noise=1e-8)
     dt = 0.25 * h
     ref = _oracle(st0, X, bbox, dt, 3)
-    got = _run("mixed", st0, X, bbox, dt, 3)
+    got = _run("mixed", st0, X, bbox, dt, 3, kernel=kernel)
     errs = [relerr(got[f], ref[f]) for f in range(24)]
     assert max(errs) <= 1e-6, errs
 
@@ -74,8 +73,7 @@ def test_graph_replay_equals_eager():
     b = e.add_block(0, (n, n, n), bbox, bbox)
     e.commit()
     e.set_state(b, st0)
-    e.enforce()
     e.run_graph(0, dt, nsteps=2, replays=2)
     assert e.sync() == 0
     assert np.array_equal(e.get_state(b), eager)
-    assert e.launches == 1 + 4 * 4
+    assert e.launches == 4 * 10   # per step: enforce pass, 4 x (stencil pass + pointwise pass), ring rotation
