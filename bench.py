@@ -2,9 +2,10 @@
 """Throughput of the BSSN RK4 evolution step on B200 (zone-updates/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-                    [--workload single64] [--impl ours|reference]
+                    [--workload amr|single64] [--kernel split|fused] [--impl ours|reference]
 
-A step is one full RK4 step (four fused substep launches) of the workload.
+A step is one Berger-Oliger coarse step of the workload (every level
+advanced to the next coarse time, with its AMR transfers).
 `value` is interior zone-updates/s with the state resident in HBM, timed with
 CUDA events on the engine's stream; `e2e` is the same metric through the
 public engine API with the state copied in from pinned host memory and back out
@@ -37,20 +38,40 @@ BYTES_PER_ZONE = {"fp64": 17 * NF * 8, "mixed": 22 * 112 + 2 * 136}
 
 
 def workload(name):
-    """Config 1: one 64^3-interior block + 3 cells each side on [-8, 8]^3,
-    Brill-Lindquist m = 1 at (0.1, 0.05, 0.02), noise 1e-8, dt = 0.25 dx."""
+    """amr: coarse 96^3 on [-48, 48]^3 (dx = 1) plus 6
+    box-in-box levels (48 cells per side per puncture, merged where their
+    buffers meet) around Brill-Lindquist punctures m = 0.5 at (+-3, 0, 0), fine
+    levels split into seeded uneven blocks; one step = one Berger-Oliger coarse
+    step (level l takes 2^l RK4 steps).
+    single64: one 64^3-interior block + 3 cells each side
+    on [-8, 8]^3, Brill-Lindquist m = 1 at (0.1, 0.05, 0.02), noise 1e-8."""
+    from amss_b200.hierarchy import box_in_box, single_block
+    if name == "amr":
+        H = box_in_box(96, 48.0, [(-3.0, 0.0, 0.0), (3.0, 0.0, 0.0)], 7, box_cells=48, seed=1,
+                       block_min=24, block_max=48)
+        return dict(H=H, masses=[0.5, 0.5], pos=[[-3.0, 0.0, 0.0], [3.0, 0.0, 0.0]], noise=0.0, eps=0.1,
+                    courant=0.25, desc="96^3 coarse on [-48,48]^3 + 6 box-in-box levels around "
+                                       "BL m=0.5 at (+-3,0,0), uneven blocks 24-48 cells, dt0=0.25 dx0; "
+                                       "step = one Berger-Oliger coarse step")
     if name == "single64":
-        return dict(n_interior=64, lo=-8.0, hi=8.0, ghosts=3, masses=[1.0], pos=[[0.1, 0.05, 0.02]],
-                    noise=1e-8, eps=0.1, courant=0.25)
+        H = single_block(64, -8.0, 8.0, 3)
+        return dict(H=H, masses=[1.0], pos=[[0.1, 0.05, 0.02]], noise=1e-8, eps=0.1, courant=0.25,
+                    desc="64^3 interior + 3 ghosts (70^3 points), one block, BL m=1 at "
+                         "(0.1,0.05,0.02), dx=0.25, dt=0.25dx, eps=0.1, noise 1e-8")
     raise SystemExit(f"unknown workload {name}")
 
 
 def make_initial(w):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # initial data only (Brill-Lindquist, get_lousto_nbhs)
-    X, st, bbox, h = O.single_block_setup(w["n_interior"], w["lo"], w["hi"], w["ghosts"], w["masses"], w["pos"],
-                                          noise=w["noise"], seed=1)
-    return X, st, bbox, h
+    import amr as OA   # initial data only (Brill-Lindquist, get_lousto_nbhs)
+    return OA.initial_state(w["H"], w["masses"], w["pos"], noise=w["noise"], seed=1)
+
+
+def counts(H):
+    """(interior zone-updates, array point-updates) of one coarse step."""
+    zones = sum(H.interior_zones(l) * 2 ** l for l in range(len(H.levels)))
+    pts = sum(H.points(l) * 2 ** l for l in range(len(H.levels)))
+    return zones, pts
 
 
 class ClockSampler:
@@ -112,7 +133,9 @@ def peaks():
 
 
 def ncu_traffic(precision):
-    """Per-launch DRAM bytes of the substep kernel from the committed ncu summary, if any."""
+    """DRAM bytes per point-step of the substep kernels (k_deriv + k_substep)
+    from the committed ncu summary, if one exists for this precision; same
+    unit as algorithmic_bytes_per_point_step."""
     p = os.path.join(ROOT, "profiles", "substep_traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
@@ -127,20 +150,18 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     w = workload(args.workload)
-    X, st0, bbox, h = make_initial(w)
-    n = len(X)
-    dt = w["courant"] * h
-    zones = w["n_interior"] ** 3          # interior zones of the block
-    npts = n ** 3                         # points the kernels update
-    eng = amss_b200.Engine(precision=args.precision, eps=w["eps"])
-    b = eng.add_block(0, (n, n, n), bbox, bbox)
-    eng.commit()
-    eng.set_state(b, st0)
+    H = w["H"]
+    init = make_initial(w)
+    dt0 = w["courant"] * H.h0
+    zones, npts = counts(H)
+    eng = amss_b200.Engine.from_hierarchy(H, precision=args.precision, eps=w["eps"], kernel=args.kernel)
+    for i, st in enumerate(init):
+        eng.set_state(i, st)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     # warm-up, then K timed steps bracketed by a barrier + synchronize
     for _ in range(args.warmup):
-        eng.step(0, dt)
+        eng.coarse_step(dt0)
     if eng.sync():
         raise SystemExit("NaN during warm-up")
     if world > 1:
@@ -150,8 +171,11 @@ def run_ours(args, rank, world):
     launches0 = eng.launches
     with ClockSampler(dev) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
-            eng.step(0, dt)
+        if args.graph:
+            eng.run_coarse_graph(dt0, nsteps=1, replays=args.steps)
+        else:
+            for _ in range(args.steps):
+                eng.coarse_step(dt0)
         ev1.record(stream)
         ev1.synchronize()
     nan = eng.sync()
@@ -165,19 +189,23 @@ def run_ours(args, rank, world):
         torch.distributed.barrier()
     ms_per_step = ms / args.steps
 
-    # end to end through the public API: pinned host state in, one step, state out
-    host_in = torch.empty(st0.shape, dtype=torch.float64, pin_memory=True).numpy()
-    host_out = torch.empty(st0.shape, dtype=torch.float64, pin_memory=True).numpy()
-    host_in[...] = st0
-    e2e_steps = max(2, min(args.steps, 10))
+    # end to end through the public API: every block's state in from pinned host
+    # memory, one coarse step, every block's state out
+    host_in = [torch.empty(st.shape, dtype=torch.float64, pin_memory=True).numpy() for st in init]
+    host_out = [torch.empty(st.shape, dtype=torch.float64, pin_memory=True).numpy() for st in init]
+    for hi, st in zip(host_in, init):
+        hi[...] = st
+    e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        eng.set_state(b, host_in)          # host -> device copy of the step's input
-        eng.step(0, dt)
-        eng.get_state(b, out=host_out)     # device -> host copy of the step's result
+        for i, hi in enumerate(host_in):
+            eng.set_state(i, hi)              # host -> device copy of the step's input
+        eng.coarse_step(dt0)
+        for i, ho in enumerate(host_out):
+            eng.get_state(i, out=ho)          # device -> host copy of the step's result
     t1 = time.perf_counter()
     e2e_ms = (t1 - t0) * 1e3 / e2e_steps
     if world > 1:
@@ -185,11 +213,11 @@ def run_ours(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
     eng.close()
+    state_bytes = int(sum(st.nbytes for st in init))
 
     value = zones * world / (ms_per_step * 1e-3)
     hbm_peak, peak_kind = peaks()
-    alg_bytes_per_step = BYTES_PER_ZONE[args.precision] * npts
-    achieved = alg_bytes_per_step / (ms_per_step * 1e-3) / 1e9
+    achieved = BYTES_PER_ZONE[args.precision] * npts / (ms_per_step * 1e-3) / 1e9
     line = {
         "metric": METRIC,
         "value": value,
@@ -202,83 +230,99 @@ def run_ours(args, rank, world):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-stencil/f64-state",
-        "data": "synthetic (Brill-Lindquist puncture + seeded 1e-8 noise, generated in-process)",
-        "config": {"workload": f"{args.workload}: 64^3 interior + 3 ghosts (70^3 points), one block, "
-                               "BL m=1 at (0.1,0.05,0.02), dx=0.25, dt=0.25dx, eps=0.1",
-                   "precision": args.precision, "zones_per_step_per_gpu": zones, "points_per_step": npts,
-                   "l2": "working set 4 x 24 x 70^3 words (>= 264 MB FP64) exceeds the 126 MB L2; no flush",
+        "data": "synthetic (Brill-Lindquist punctures, generated in-process)",
+        "config": {"workload": f"{args.workload}: {w['desc']}",
+                   "precision": args.precision, "kernel": args.kernel, "graph": bool(args.graph),
+                   "zone_updates_per_step_per_gpu": zones, "point_updates_per_step": npts,
+                   "levels": len(H.levels), "blocks": len(H.blocks),
+                   "l2": "state + stages + K of the hierarchy (GBs) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{world} (no data-path collective)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
                      "traffic": ncu_traffic(args.precision),
-                     "kernel": "k_substep (fused RHS + RK4 substep)",
+                     "traffic_unit": "B/point-step",
+                     "kernel": "whole coarse step: RK4 substeps (stencil pass + pointwise pass) and the AMR "
+                               "transfers, timed together",
                      "algorithmic_bytes_per_point_step": BYTES_PER_ZONE[args.precision]},
         "e2e": {"value": zones * world / (e2e_ms * 1e-3), "unit": "zone-updates/s",
-                "h2d_bytes_per_step": int(st0.nbytes), "d2h_bytes_per_step": int(st0.nbytes),
-                "path": "amss_b200.Engine set_state (pinned) -> step -> get_state"},
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "path": "amss_b200.Engine set_state (pinned, every block) -> coarse_step -> get_state"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "nan": bool(nan),
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, w)
+        line["cpu_baseline"] = cpu_baseline(args, w, init)
     return line
 
 
-def cpu_baseline(args, w, budget_s=12.0):
-    """The oracle (C restatement of the reference's Fortran, OpenMP over k) on
-    the host cores: RK4 steps of the full config-1 block until ~budget_s."""
+def _oracle_sample(w, init, budget_s):
+    """Time the oracle (C restatement of the reference's Fortran, OpenMP over
+    k) on RK4 steps of the finest level until about budget_s have passed."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    X, st, bbox, h = make_initial(w)
-    dt = w["courant"] * h
-    O.bssn_step_single(X, X, X, bbox, st, dt, eps=w["eps"])   # warm-up
+    import amr as OA
+    H = w["H"]
+    oh = OA.OracleHierarchy(H, eps=w["eps"])
+    for i, st in enumerate(init):
+        oh.set_state(i, st)
+    lev = len(H.levels) - 1
+    dt = w["courant"] * H.h(lev)
+    oh.level_step(lev, dt)       # warm-up
     t0 = time.perf_counter()
     steps = 0
     while True:
-        O.bssn_step_single(X, X, X, bbox, st, dt, eps=w["eps"])
+        oh.level_step(lev, dt)
         steps += 1
         if time.perf_counter() - t0 > budget_s:
             break
-    dt_s = time.perf_counter() - t0
-    zones = w["n_interior"] ** 3
+    el = time.perf_counter() - t0
+    return H.interior_zones(lev) * steps / el, steps, lev
+
+
+def cpu_baseline(args, w, init, budget_s=12.0):
+    v, steps, lev = _oracle_sample(w, init, budget_s)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
-    return {"value": zones * steps / dt_s, "unit": "zone-updates/s", "cores": cores, "kind": "port",
-            "sample": f"{steps} RK4 step(s) of the full 70^3 config-1 block, FP64, OpenMP over {cores} threads"}
+    return {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} RK4 step(s) of level {lev} of the workload ({w['H'].interior_zones(lev)} interior "
+                      f"zones), FP64, OpenMP over {cores} threads"}
 
 
 def run_reference(args, rank, world):
-    """The reference arm: one RK4 step of the config-1 block per bench step,
-    run by the oracle (the C restatement of the reference's Fortran) on all
-    host cores.  Only rank 0 works under torchrun."""
+    """The reference arm: the oracle (the C restatement of the reference's
+    Fortran) on all host cores, one finest-level RK4 step of the workload per
+    bench step.  Only rank 0 works under torchrun."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    import amr as OA
     w = workload(args.workload)
-    X, st, bbox, h = make_initial(w)
-    dt = w["courant"] * h
+    H = w["H"]
+    init = make_initial(w)
+    oh = OA.OracleHierarchy(H, eps=w["eps"])
+    for i, st in enumerate(init):
+        oh.set_state(i, st)
+    lev = len(H.levels) - 1
+    dt = w["courant"] * H.h(lev)
     for _ in range(args.warmup):
-        O.bssn_step_single(X, X, X, bbox, st, dt, eps=w["eps"])
+        oh.level_step(lev, dt)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.bssn_step_single(X, X, X, bbox, st, dt, eps=w["eps"])
+        oh.level_step(lev, dt)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * sum(times) / len(times)
-    zones = w["n_interior"] ** 3
-    v = zones / (ms * 1e-3)
+    v = H.interior_zones(lev) / (ms * 1e-3)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: 64^3 interior + 3 ghosts, one block (as the GPU arm)",
-                   "precision": "fp64"},
+        "config": {"workload": f"{args.workload}: {w['desc']}", "precision": "fp64",
+                   "sample": f"one RK4 step of level {lev} per bench step"},
         "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
-                         "sample": "one RK4 step of the full 70^3 config-1 block per bench step: the C "
-                                   "restatement of the reference's Fortran (oracle/), OpenMP over k; the "
-                                   "Fortran itself cannot be compiled in this image"},
+                         "sample": f"one RK4 step of level {lev} of the workload per bench step: the C restatement "
+                                   "of the reference's Fortran (oracle/), OpenMP over k; the Fortran itself cannot "
+                                   "be compiled in this image"},
         "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -286,10 +330,12 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--workload", default="single64")
+    ap.add_argument("--workload", choices=["amr", "single64"], default="amr")
+    ap.add_argument("--kernel", choices=["split", "fused"], default="split")
+    ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
