@@ -71,6 +71,38 @@ int compute_rhs_bssn_(
     double* Gmx_Res, double* Gmy_Res, double* Gmz_Res,
     int* Symmetry, int* Lev, double* eps, int* co);
 
+/* No counterpart in the reference.  compute_rhs_bssn_ for callers that cannot
+ * allocate device memory (a host inside a memory pool it does not own, or one
+ * whose device memory is reserved up front): same arguments, outputs and NaN
+ * rule, but no cudaMalloc/cudaFree and no stream creation.  Its device staging
+ * area is a static array of the library (23.4 MB per device) that every call
+ * shares, so blocks are limited to AMSS_NOALLOC_MAX_POINTS points (and 4096
+ * per extent; larger ones fail with AMSS_ERR_ARG), and calls that overlap on
+ * the GPU race: serialise them.  Runs on the per-thread default stream. */
+#define AMSS_NOALLOC_MAX_POINTS 32768
+int amss_compute_rhs_bssn_noalloc(
+    int* ex, double* T, double* X, double* Y, double* Z,
+    double* chi, double* trK, double* dxx, double* gxy, double* gxz, double* dyy, double* gyz, double* dzz,
+    double* Axx, double* Axy, double* Axz, double* Ayy, double* Ayz, double* Azz,
+    double* Gamx, double* Gamy, double* Gamz,
+    double* Lap, double* betax, double* betay, double* betaz,
+    double* dtSfx, double* dtSfy, double* dtSfz,
+    double* chi_rhs, double* trK_rhs,
+    double* gxx_rhs, double* gxy_rhs, double* gxz_rhs, double* gyy_rhs, double* gyz_rhs, double* gzz_rhs,
+    double* Axx_rhs, double* Axy_rhs, double* Axz_rhs, double* Ayy_rhs, double* Ayz_rhs, double* Azz_rhs,
+    double* Gamx_rhs, double* Gamy_rhs, double* Gamz_rhs,
+    double* Lap_rhs, double* betax_rhs, double* betay_rhs, double* betaz_rhs,
+    double* dtSfx_rhs, double* dtSfy_rhs, double* dtSfz_rhs,
+    double* rho, double* Sx, double* Sy, double* Sz,
+    double* Sxx, double* Sxy, double* Sxz, double* Syy, double* Syz, double* Szz,
+    double* Gamxxx, double* Gamxxy, double* Gamxxz, double* Gamxyy, double* Gamxyz, double* Gamxzz,
+    double* Gamyxx, double* Gamyxy, double* Gamyxz, double* Gamyyy, double* Gamyyz, double* Gamyzz,
+    double* Gamzxx, double* Gamzxy, double* Gamzxz, double* Gamzyy, double* Gamzyz, double* Gamzzz,
+    double* Rxx, double* Rxy, double* Rxz, double* Ryy, double* Ryz, double* Rzz,
+    double* ham_Res, double* movx_Res, double* movy_Res, double* movz_Res,
+    double* Gmx_Res, double* Gmy_Res, double* Gmz_Res,
+    int* Symmetry, int* Lev, double* eps, int* co);
+
 /* Replaces rungekutta4_rout (rungekutta4_rout.f90:94-139; rungekutta4_rout.h:34-38,
  * called per field from bssn_class.C:3119 and :3430-3525).  RK4 = 0..3. */
 int rungekutta4_rout_(int* ex, double* dT, double* f0, double* f1, double* f_rhs, int* RK4);

@@ -58,6 +58,26 @@ def compute_rhs_bssn(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, co
     return gont, rhs, gam, ric, cons
 
 
+def compute_rhs_bssn_noalloc(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, co=1, T=0.0):
+    """compute_rhs_bssn through amss_compute_rhs_bssn_noalloc: the same
+    kernel with no device allocation; blocks of at most
+    AMSS_NOALLOC_MAX_POINTS (32768) points; calls must not overlap.  Same
+    return value as compute_rhs_bssn."""
+    state = np.ascontiguousarray(state, dtype=np.float64)
+    shp = state.shape[1:]
+    out = [np.zeros((k,) + shp) for k in (24, 18, 6, 7)]
+    matter = np.zeros((10,) + shp) if matter is None else np.ascontiguousarray(matter, dtype=np.float64)
+    X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
+    args = [_ex(shp), ctypes.byref(ctypes.c_double(T)), _p(X), _p(Y), _p(Z)]
+    args += [_p(state[f]) for f in range(24)] + [_p(out[0][f]) for f in range(24)]
+    args += [_p(matter[f]) for f in range(10)]
+    args += [_p(a[f]) for a in out[1:] for f in range(a.shape[0])]
+    args += [ctypes.byref(ctypes.c_int(symmetry)), ctypes.byref(ctypes.c_int(lev)),
+             ctypes.byref(ctypes.c_double(eps)), ctypes.byref(ctypes.c_int(co))]
+    gont = check(lib().amss_compute_rhs_bssn_noalloc(*args), "amss_compute_rhs_bssn_noalloc")
+    return (gont,) + tuple(out)
+
+
 def rungekutta4_rout(dT, f0, f1, f_rhs, rk4):
     """rungekutta4_rout (rungekutta4_rout.f90:94-139), f1 and f_rhs in place."""
     return check(lib().rungekutta4_rout_(_ex(f0.shape), ctypes.byref(ctypes.c_double(dT)), _p(f0), _p(f1),
