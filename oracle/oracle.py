@@ -93,6 +93,33 @@ def compute_rhs_bssn(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, co
     return gont, rhs, gam, ric, cons
 
 
+def compute_rhs_z4c(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, T=0.0):
+    """Z4c_rhs.f90:126-1295 (state of 25 fields, Theta last).  Returns
+    (gont, rhs[25], gamma[18], ricci[6], cons[7]); the constraints are always
+    computed (the Fortran ignores co)."""
+    state = np.ascontiguousarray(state, dtype=np.float64)
+    shp = state.shape[1:]
+    ex = _ex(shp)
+    rhs = np.zeros((25,) + shp)
+    gam = np.zeros((18,) + shp)
+    ric = np.zeros((6,) + shp)
+    cons = np.zeros((7,) + shp)
+    if matter is None:
+        matter = np.zeros((10,) + shp)
+    matter = np.ascontiguousarray(matter, dtype=np.float64)
+    X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
+    args = [ex, ctypes.c_double(T), _p(X), _p(Y), _p(Z)]
+    args += [_p(state[f]) for f in range(25)]
+    args += [_p(rhs[f]) for f in range(25)]
+    args += [_p(matter[f]) for f in range(10)]
+    args += [_p(gam[f]) for f in range(18)]
+    args += [_p(ric[f]) for f in range(6)]
+    args += [_p(cons[f]) for f in range(7)]
+    args += [ctypes.c_int(symmetry), ctypes.c_int(lev), ctypes.c_double(eps), ctypes.c_int(0)]
+    gont = lib().oracle_compute_rhs_z4c(*args)
+    return gont, rhs, gam, ric, cons
+
+
 def fderivs(X, Y, Z, f, soa=(1.0, 1.0, 1.0), symmetry=0):
     f = np.ascontiguousarray(f, dtype=np.float64)
     out = [np.zeros_like(f) for _ in range(3)]
