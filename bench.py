@@ -30,11 +30,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "nr-amssncku_b200"))
 
 METRIC = "BSSN RK4 zone-updates/s on 1 B200: FP64 vs mixed, %HBM peak; adjoint/fwd ratio"
-NF = 24
 # algorithmic HBM bytes per zone-update: every field array read or written once per
-# substep, 17 words per field per step.  Mixed: FP32 stages for 22 fields, FP64
-# stages for chi and alpha, FP64 U0/K/U_new: 22 * 112 + 2 * 136.
-BYTES_PER_ZONE = {"fp64": 17 * NF * 8, "mixed": 22 * 112 + 2 * 136}
+# substep, 17 words per field per step.  Mixed: FP32 stages for all but chi and
+# alpha, FP64 stages for those two, FP64 U0/K/U_new: (nf - 2) * 112 + 2 * 136.
+def bytes_per_zone(precision, nf):
+    return 17 * nf * 8 if precision == "fp64" else (nf - 2) * 112 + 2 * 136
 
 
 def workload(name):
@@ -47,24 +47,32 @@ def workload(name):
     on [-8, 8]^3, Brill-Lindquist m = 1 at (0.1, 0.05, 0.02), noise 1e-8."""
     from amss_b200.hierarchy import box_in_box, single_block
     if name == "amr":
+        # blocks of 24^3 to 80^3 points: 18 to 74 cells plus 3 ghost cells a side
         H = box_in_box(96, 48.0, [(-3.0, 0.0, 0.0), (3.0, 0.0, 0.0)], 7, box_cells=48, seed=1,
-                       block_min=24, block_max=48)
+                       block_min=18, block_max=74)
         return dict(H=H, masses=[0.5, 0.5], pos=[[-3.0, 0.0, 0.0], [3.0, 0.0, 0.0]], noise=0.0, eps=0.1,
                     courant=0.25, desc="96^3 coarse on [-48,48]^3 + 6 box-in-box levels around "
-                                       "BL m=0.5 at (+-3,0,0), uneven blocks 24-48 cells, dt0=0.25 dx0; "
+                                       "BL m=0.5 at (+-3,0,0), uneven blocks of 24^3-80^3 points, dt0=0.25 dx0; "
                                        "step = one Berger-Oliger coarse step")
-    if name == "single64":
-        H = single_block(64, -8.0, 8.0, 3)
+    if name == "amr8":
+        H = box_in_box(96, 48.0, [(0.1, 0.05, 0.02)], 8, box_cells=64, seed=1, block_min=48, block_max=160)
         return dict(H=H, masses=[1.0], pos=[[0.1, 0.05, 0.02]], noise=1e-8, eps=0.1, courant=0.25,
-                    desc="64^3 interior + 3 ghosts (70^3 points), one block, BL m=1 at "
-                         "(0.1,0.05,0.02), dx=0.25, dt=0.25dx, eps=0.1, noise 1e-8")
+                    desc="96^3 coarse on [-48,48]^3 + 7 box-in-box levels of 64^3 cells around BL m=1 at "
+                         "(0.1,0.05,0.02), blocks 48-160 cells, dt0=0.25 dx0, noise 1e-8; step = one "
+                         "Berger-Oliger coarse step")
+    if name.startswith("single") and name[6:].isdigit():
+        n = int(name[6:])
+        H = single_block(n, -n / 8.0, n / 8.0, 3)
+        return dict(H=H, masses=[1.0], pos=[[0.1, 0.05, 0.02]], noise=1e-8, eps=0.1, courant=0.25,
+                    desc=f"{n}^3 interior + 3 ghosts ({n + 6}^3 points), one block on [-{n / 8:g},{n / 8:g}]^3, "
+                         "BL m=1 at (0.1,0.05,0.02), dx=0.25, dt=0.25dx, eps=0.1, noise 1e-8")
     raise SystemExit(f"unknown workload {name}")
 
 
-def make_initial(w):
+def make_initial(w, nf=24):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import amr as OA   # initial data only (Brill-Lindquist, get_lousto_nbhs)
-    return OA.initial_state(w["H"], w["masses"], w["pos"], noise=w["noise"], seed=1)
+    return OA.initial_state(w["H"], w["masses"], w["pos"], noise=w["noise"], seed=1, nf=nf)
 
 
 def counts(H):
@@ -132,14 +140,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(precision):
+def ncu_traffic(precision, formulation):
     """DRAM bytes per point-step of the substep kernels (k_deriv + k_substep)
-    from the committed ncu summary, if one exists for this precision; same
-    unit as algorithmic_bytes_per_point_step."""
+    from the committed ncu summary, if one exists for this precision and
+    formulation; same unit as algorithmic_bytes_per_point_step."""
     p = os.path.join(ROOT, "profiles", "substep_traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get(precision)
+        return d.get(precision if formulation == "bssn" else f"z4c_{precision}")
     return None
 
 
@@ -151,10 +159,12 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     w = workload(args.workload)
     H = w["H"]
-    init = make_initial(w)
+    nf = 25 if args.formulation == "z4c" else 24
+    init = make_initial(w, nf)
     dt0 = w["courant"] * H.h0
     zones, npts = counts(H)
-    eng = amss_b200.Engine.from_hierarchy(H, precision=args.precision, eps=w["eps"], kernel=args.kernel)
+    eng = amss_b200.Engine.from_hierarchy(H, precision=args.precision, eps=w["eps"], kernel=args.kernel,
+                                          formulation=args.formulation)
     for i, st in enumerate(init):
         eng.set_state(i, st)
     stream = torch.cuda.ExternalStream(eng.stream)
@@ -217,7 +227,8 @@ def run_ours(args, rank, world):
 
     value = zones * world / (ms_per_step * 1e-3)
     hbm_peak, peak_kind = peaks()
-    achieved = BYTES_PER_ZONE[args.precision] * npts / (ms_per_step * 1e-3) / 1e9
+    bpz = bytes_per_zone(args.precision, nf)
+    achieved = bpz * npts / (ms_per_step * 1e-3) / 1e9
     line = {
         "metric": METRIC,
         "value": value,
@@ -231,7 +242,7 @@ def run_ours(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-stencil/f64-state",
         "data": "synthetic (Brill-Lindquist punctures, generated in-process)",
-        "config": {"workload": f"{args.workload}: {w['desc']}",
+        "config": {"workload": f"{args.workload}: {w['desc']}", "formulation": args.formulation,
                    "precision": args.precision, "kernel": args.kernel, "graph": bool(args.graph),
                    "zone_updates_per_step_per_gpu": zones, "point_updates_per_step": npts,
                    "levels": len(H.levels), "blocks": len(H.blocks),
@@ -239,11 +250,11 @@ def run_ours(args, rank, world):
                    "parallelism": f"replicas x{world} (no data-path collective)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": ncu_traffic(args.precision),
+                     "traffic": ncu_traffic(args.precision, args.formulation),
                      "traffic_unit": "B/point-step",
                      "kernel": "whole coarse step: RK4 substeps (stencil pass + pointwise pass) and the AMR "
                                "transfers, timed together",
-                     "algorithmic_bytes_per_point_step": BYTES_PER_ZONE[args.precision]},
+                     "algorithmic_bytes_per_point_step": bpz},
         "e2e": {"value": zones * world / (e2e_ms * 1e-3), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "path": "amss_b200.Engine set_state (pinned, every block) -> coarse_step -> get_state"},
@@ -262,7 +273,7 @@ def _oracle_sample(w, init, budget_s):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import amr as OA
     H = w["H"]
-    oh = OA.OracleHierarchy(H, eps=w["eps"])
+    oh = OA.OracleHierarchy(H, eps=w["eps"], nf=init[0].shape[0])
     for i, st in enumerate(init):
         oh.set_state(i, st)
     lev = len(H.levels) - 1
@@ -297,8 +308,9 @@ def run_reference(args, rank, world):
     import amr as OA
     w = workload(args.workload)
     H = w["H"]
-    init = make_initial(w)
-    oh = OA.OracleHierarchy(H, eps=w["eps"])
+    nf = 25 if args.formulation == "z4c" else 24
+    init = make_initial(w, nf)
+    oh = OA.OracleHierarchy(H, eps=w["eps"], nf=nf)
     for i, st in enumerate(init):
         oh.set_state(i, st)
     lev = len(H.levels) - 1
@@ -317,7 +329,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: {w['desc']}", "precision": "fp64",
+        "config": {"workload": f"{args.workload}: {w['desc']}", "formulation": args.formulation,
+                   "precision": "fp64",
                    "sample": f"one RK4 step of level {lev} per bench step"},
         "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                          "sample": f"one RK4 step of level {lev} of the workload per bench step: the C restatement "
@@ -333,7 +346,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--workload", choices=["amr", "single64"], default="amr")
+    ap.add_argument("--workload", default="amr",
+                    help="amr | amr8 | singleN (one block of N^3 interior cells, e.g. single64, single320)")
+    ap.add_argument("--formulation", choices=["bssn", "z4c"], default="bssn")
     ap.add_argument("--kernel", choices=["split", "fused"], default="split")
     ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")

@@ -71,6 +71,37 @@ int compute_rhs_bssn_(
     double* Gmx_Res, double* Gmy_Res, double* Gmz_Res,
     int* Symmetry, int* Lev, double* eps, int* co);
 
+/* Replaces compute_rhs_Z4c (Z4c_rhs.f90:126-1295; C prototype bssn_rhs.h:142-160,
+ * called per block from Z4c_class.C:207 and :575).  GAUGE 0, Cell, ghost_width 3,
+ * kappa1 = 0.02, kappa2 = 0 (cpbc.f90:5-20).  State and RHS lists as
+ * compute_rhs_bssn_ with Theta (TZ) after dtSfz.  The diagnostic outputs
+ * (physical Christoffels, Ricci, the 7 constraint residuals) are always
+ * computed, from the first 24 fields, as ricci_gamma and constraint_bssn do
+ * (Z4c_rhs.f90:1266-1290); co is ignored.  Returns 1 without touching any
+ * output when one of the 25 state fields holds a NaN (Z4c_rhs.f90:230-262). */
+int compute_rhs_z4c_(
+    int* ex, double* T, double* X, double* Y, double* Z,
+    double* chi, double* trK, double* dxx, double* gxy, double* gxz, double* dyy, double* gyz, double* dzz,
+    double* Axx, double* Axy, double* Axz, double* Ayy, double* Ayz, double* Azz,
+    double* Gamx, double* Gamy, double* Gamz,
+    double* Lap, double* betax, double* betay, double* betaz,
+    double* dtSfx, double* dtSfy, double* dtSfz, double* TZ,
+    double* chi_rhs, double* trK_rhs,
+    double* gxx_rhs, double* gxy_rhs, double* gxz_rhs, double* gyy_rhs, double* gyz_rhs, double* gzz_rhs,
+    double* Axx_rhs, double* Axy_rhs, double* Axz_rhs, double* Ayy_rhs, double* Ayz_rhs, double* Azz_rhs,
+    double* Gamx_rhs, double* Gamy_rhs, double* Gamz_rhs,
+    double* Lap_rhs, double* betax_rhs, double* betay_rhs, double* betaz_rhs,
+    double* dtSfx_rhs, double* dtSfy_rhs, double* dtSfz_rhs, double* TZ_rhs,
+    double* rho, double* Sx, double* Sy, double* Sz,
+    double* Sxx, double* Sxy, double* Sxz, double* Syy, double* Syz, double* Szz,
+    double* Gamxxx, double* Gamxxy, double* Gamxxz, double* Gamxyy, double* Gamxyz, double* Gamxzz,
+    double* Gamyxx, double* Gamyxy, double* Gamyxz, double* Gamyyy, double* Gamyyz, double* Gamyzz,
+    double* Gamzxx, double* Gamzxy, double* Gamzxz, double* Gamzyy, double* Gamzyz, double* Gamzzz,
+    double* Rxx, double* Rxy, double* Rxz, double* Ryy, double* Ryz, double* Rzz,
+    double* Hcon, double* Mxcon, double* Mycon, double* Mzcon,
+    double* Gmxcon, double* Gmycon, double* Gmzcon,
+    int* Symmetry, int* Lev, double* eps, int* co);
+
 /* No counterpart in the reference.  compute_rhs_bssn_ for callers that cannot
  * allocate device memory (a host inside a memory pool it does not own, or one
  * whose device memory is reserved up front): same arguments, outputs and NaN
@@ -143,6 +174,8 @@ typedef struct {
   double eps;         /* KO dissipation (ABE::... dissipation) */
   double chitiny;     /* chi floor as the reference stores it: BSSN::chitiny - 1 */
   int kernel;         /* 0: split substep (stencil pass + pointwise pass, default); 1: fused single pass */
+  int formulation;    /* 0: BSSN, 24 fields (bssn_rhs.f90); 1: Z4c, 25 fields with Theta last
+                         (Z4c_rhs.f90:126-1295, ABEtype 2); Z4c needs kernel 0 */
 } amss_params;
 
 /* Create an engine on the current CUDA device.  Returns NULL on failure. */

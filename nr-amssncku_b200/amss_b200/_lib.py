@@ -29,6 +29,7 @@ def lib():
     L.amss_last_error.restype = ctypes.c_char_p
     L.amss_version.restype = ctypes.c_char_p
     L.compute_rhs_bssn_.restype = ctypes.c_int
+    L.compute_rhs_z4c_.restype = ctypes.c_int
     L.amss_compute_rhs_bssn_noalloc.restype = ctypes.c_int
     L.rungekutta4_rout_.restype = ctypes.c_int
     for name in ("sommerfeld_routbam_", "sommerfeld_rout_", "enforce_ga_", "lowerboundset_"):

@@ -58,6 +58,25 @@ def compute_rhs_bssn(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, co
     return gont, rhs, gam, ric, cons
 
 
+def compute_rhs_z4c(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, T=0.0):
+    """compute_rhs_Z4c (Z4c_rhs.f90:126-1295) on the GPU; state of 25 fields
+    (Theta last).  Returns (gont, rhs[25], gamma[18], ricci[6], cons[7]); the
+    constraints are always computed."""
+    state = np.ascontiguousarray(state, dtype=np.float64)
+    shp = state.shape[1:]
+    out = [np.zeros((k,) + shp) for k in (25, 18, 6, 7)]
+    matter = np.zeros((10,) + shp) if matter is None else np.ascontiguousarray(matter, dtype=np.float64)
+    X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
+    args = [_ex(shp), ctypes.byref(ctypes.c_double(T)), _p(X), _p(Y), _p(Z)]
+    args += [_p(state[f]) for f in range(25)] + [_p(out[0][f]) for f in range(25)]
+    args += [_p(matter[f]) for f in range(10)]
+    args += [_p(a[f]) for a in out[1:] for f in range(a.shape[0])]
+    args += [ctypes.byref(ctypes.c_int(symmetry)), ctypes.byref(ctypes.c_int(lev)),
+             ctypes.byref(ctypes.c_double(eps)), ctypes.byref(ctypes.c_int(0))]
+    gont = check(lib().compute_rhs_z4c_(*args), "compute_rhs_z4c_")
+    return (gont,) + tuple(out)
+
+
 def compute_rhs_bssn_noalloc(X, Y, Z, state, matter=None, symmetry=0, lev=0, eps=0.1, co=1, T=0.0):
     """compute_rhs_bssn through amss_compute_rhs_bssn_noalloc: the same
     kernel with no device allocation; blocks of at most

@@ -13,7 +13,8 @@ from ._lib import _DP, AmssError, check, last_error, lib
 
 class _Params(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("symmetry", ctypes.c_int),
-                ("eps", ctypes.c_double), ("chitiny", ctypes.c_double), ("kernel", ctypes.c_int)]
+                ("eps", ctypes.c_double), ("chitiny", ctypes.c_double), ("kernel", ctypes.c_int),
+                ("formulation", ctypes.c_int)]
 
 
 class Engine:
@@ -23,10 +24,16 @@ class Engine:
     accumulator and update).  kernel: "split" (a stencil pass through shared
     memory, then the pointwise RHS and RK4 update) or "fused" (one pass,
     every stencil from global memory).  chitiny is BSSN::chitiny as the par file gives
-    it (1e-5); the engine shifts it by -1 as bssn_class.C:179 does."""
+    it (1e-5); the engine shifts it by -1 as bssn_class.C:179 does.
+    formulation: "bssn" (24 fields) or "z4c" (25 fields, Theta last; split
+    kernel only)."""
 
-    def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5, kernel="split"):
-        prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0, 0 if kernel == "split" else 1)
+    def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5, kernel="split", formulation="bssn"):
+        if formulation not in ("bssn", "z4c"):
+            raise AmssError("formulation must be 'bssn' or 'z4c'")
+        self.nf = 25 if formulation == "z4c" else 24
+        prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0, 0 if kernel == "split" else 1,
+                      1 if formulation == "z4c" else 0)
         self._h = lib().amss_engine_create(ctypes.byref(prm))
         if not self._h:
             raise AmssError("amss_engine_create failed: " + last_error())
@@ -90,14 +97,17 @@ class Engine:
 
     def set_state(self, block, state):
         state = np.ascontiguousarray(state, dtype=np.float64)
+        ex = self.blocks[block]
+        if state.shape != (self.nf, ex[2], ex[1], ex[0]):
+            raise AmssError(f"set_state: state must have shape {(self.nf, ex[2], ex[1], ex[0])}, got {state.shape}")
         check(lib().amss_engine_set_state(self._h, block, state.ctypes.data_as(_DP)), "amss_engine_set_state")
 
     def get_state(self, block, out=None):
         ex = self.blocks[block]
         if out is None:
-            out = np.empty((24, ex[2], ex[1], ex[0]))
-        if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (24, ex[2], ex[1], ex[0]):
-            raise AmssError("get_state: out must be a C-contiguous float64 (24, ez, ey, ex) array")
+            out = np.empty((self.nf, ex[2], ex[1], ex[0]))
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (self.nf, ex[2], ex[1], ex[0]):
+            raise AmssError(f"get_state: out must be a C-contiguous float64 ({self.nf}, ez, ey, ex) array")
         check(lib().amss_engine_get_state(self._h, block, out.ctypes.data_as(_DP)), "amss_engine_get_state")
         return out
 

@@ -4,7 +4,7 @@
 // Every operation is a list of boxes in global level indices; a box names a
 // destination block and a source block.  Threads are mapped to box points
 // through a tile list (128 points per tile), so one launch serves all boxes
-// of a level, whatever their sizes.  Each thread moves all 24 fields of one
+// of a level, whatever their sizes.  Each thread moves all nf fields of one
 // point.  Nothing here applies enforce_ga: as in the reference, restricted and
 // prolonged values are enforced by the pass at the start of the next step.
 #pragma once
@@ -21,7 +21,7 @@ __device__ __forceinline__ bool amr_inside(const AmrBlock& b, int gi, int gj, in
 }
 __device__ __forceinline__ double* amr_state(const AmrBlock& b) { return b.tl[b.lvl[0]]; }
 
-// Same-level ghost fill: copy the 24 fields of each box point from src to dst.
+// Same-level ghost fill: copy the nf fields of each box point from src to dst.
 template <typename SS>
 __global__ void k_amr_sync(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
                            const int2* __restrict__ tiles, int ntiles, int which, unsigned* status) {
@@ -39,12 +39,12 @@ __global__ void k_amr_sync(const AmrBlock* __restrict__ blocks, const AmrBox* __
     if (which == BUF_STATE || which == BUF_TEMP) {
       const double* s = which == BUF_STATE ? amr_state(S) : S.K;
       double* d = which == BUF_STATE ? amr_state(D) : D.K;
-      for (int f = 0; f < 24; ++f) d[f * D.fs + od] = s[f * S.fs + os];
+      for (int f = 0; f < D.nf; ++f) d[f * D.fs + od] = s[f * S.fs + os];
     } else {
       const int sl = which == BUF_STAGE_A ? 0 : 1;
       const SS* s = (const SS*)S.st[sl];
       SS* d = (SS*)D.st[sl];
-      for (int f = 0; f < 24; ++f) d[f * D.fs + od] = s[f * S.fs + os];
+      for (int f = 0; f < D.nf; ++f) d[f * D.fs + od] = s[f * S.fs + os];
       if constexpr (sizeof(SS) == 4) {
         D.side[sl][od] = S.side[sl][os];
         D.side[sl][D.fs + od] = S.side[sl][S.fs + os];
@@ -91,8 +91,8 @@ __global__ void k_amr_prolong(const AmrBlock* __restrict__ blocks, const AmrBox*
     double w[3][6];
     for (int d = 0; d < 3; ++d)
       for (int m = 0; m < 6; ++m) w[d][m] = kProlongW[rev[d] ? 5 - m : m];
-    double out[24];
-    for (int f = 0; f < 24; ++f) {
+    double out[NFIELDS_Z4C];
+    for (int f = 0; f < D.nf; ++f) {
       const double* q = src + f * S.fs + base;
       double tmp1[6];
       for (int a = 0; a < 6; ++a) {
@@ -112,7 +112,7 @@ __global__ void k_amr_prolong(const AmrBlock* __restrict__ blocks, const AmrBox*
     if (enforce) enforce_ga_point(out + F_GXX, out + F_AXX);  // off on the evolution path
     double* dst = amr_state(D);
     const long long od = amr_idx(D, g[0], g[1], g[2]);
-    for (int f = 0; f < 24; ++f) dst[f * D.fs + od] = out[f];
+    for (int f = 0; f < D.nf; ++f) dst[f * D.fs + od] = out[f];
   }
 }
 
@@ -141,8 +141,8 @@ __global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox
     const double* src = amr_state(S);
     const long long sy = S.ex[0], sz = (long long)S.ex[0] * S.ex[1];
     const long long base = amr_idx(S, f0[0], f0[1], f0[2]);
-    double out[24];
-    for (int f = 0; f < 24; ++f) {
+    double out[NFIELDS_Z4C];
+    for (int f = 0; f < D.nf; ++f) {
       const double* q = src + f * S.fs + base;
       double tmp1[6];
       for (int a = 0; a < 6; ++a) {
@@ -160,10 +160,10 @@ __global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox
     }
     const long long od = amr_idx(D, c[0], c[1], c[2]);
     if (to_temp) {
-      for (int f = 0; f < 24; ++f) D.K[f * D.fs + od] = out[f];
+      for (int f = 0; f < D.nf; ++f) D.K[f * D.fs + od] = out[f];
     } else {
       double* dst = amr_state(D);
-      for (int f = 0; f < 24; ++f) dst[f * D.fs + od] = out[f];
+      for (int f = 0; f < D.nf; ++f) dst[f * D.fs + od] = out[f];
     }
   }
 }
@@ -185,12 +185,12 @@ __global__ void k_amr_timeinterp(const AmrBlock* __restrict__ blocks, const int2
     const double* f3 = B.tl[(cur + 1) % 3];
     if (B.lvl[1] >= 2) {
       const double C1 = 3.0 / 8.0, C2 = 3.0 / 4.0, C3 = -1.0 / 8.0;
-      for (int f = 0; f < 24; ++f) {
+      for (int f = 0; f < B.nf; ++f) {
         const long long o = f * B.fs + p;
         B.K[o] = __dadd_rn(__dadd_rn(__dmul_rn(C1, f1[o]), __dmul_rn(C2, f2[o])), __dmul_rn(C3, f3[o]));
       }
     } else {
-      for (int f = 0; f < 24; ++f) {
+      for (int f = 0; f < B.nf; ++f) {
         const long long o = f * B.fs + p;
         B.K[o] = __dmul_rn(0.5, __dadd_rn(f1[o], f2[o]));
       }

@@ -14,6 +14,7 @@ struct AmrBlock {
   double* side[2];     // FP64 chi, alpha of the stages (mixed form)
   double* K;           // RK accumulator, reused as the time-interpolated parent state
   const int* lvl;      // level state {cur, steps taken}
+  int nf;              // evolved fields: 24 (BSSN) or 25 (Z4c)
 };
 
 // A box of work: [lo, lo + n) in global level indices of the destination.

@@ -10,7 +10,19 @@
 // g~ii-1), as the reference stores them.
 #pragma once
 #include <cstdint>
+#ifndef AMSS_HOST_TRACE
 #include <cuda_runtime.h>
+#else
+// host compile of the point functions for the adjoint generator (gen/)
+#define __device__
+#define __host__
+#define __forceinline__ inline
+template <typename T>
+inline T __ldg(const T* p) { return *p; }
+inline double __dadd_rn(double a, double b) { return a + b; }
+inline double __dsub_rn(double a, double b) { return a - b; }
+inline double __dmul_rn(double a, double b) { return a * b; }
+#endif
 
 namespace amss {
 
@@ -28,6 +40,7 @@ enum StatusBits : unsigned {
   ST_PINF = 2u,       // +inf seen in a checked input field
   ST_NINF = 4u,       // -inf seen in a checked input field
   ST_BAD_ARG = 8u,    // a kernel was handed an inconsistent descriptor
+  ST_TIMEOUT = 16u,   // a bounded wait on an asynchronous copy gave up
 };
 
 // Parity of each state field under reflection x, y, z (bssn_class.C:177-330).

@@ -18,6 +18,16 @@
 
 namespace amss {
 
+// instantiated in rhs_dropin*.cu
+extern template cudaError_t launch_rhs_dropin<false>(int, cudaStream_t, BlockView, Coefs<double>, const double*,
+                                                     double*, RhsAux, unsigned*);
+extern template cudaError_t launch_rhs_dropin<true>(int, cudaStream_t, BlockView, Coefs<double>, const double*,
+                                                    double*, RhsAux, unsigned*);
+extern template cudaError_t launch_rhs_dropin_z4c<false>(int, cudaStream_t, BlockView, Coefs<double>, const double*,
+                                                         double*, const double*, unsigned*);
+extern template cudaError_t launch_rhs_dropin_z4c<true>(int, cudaStream_t, BlockView, Coefs<double>, const double*,
+                                                        double*, const double*, unsigned*);
+
 // -----------------------------------------------------------------------------
 // Kernels
 // -----------------------------------------------------------------------------
@@ -289,6 +299,96 @@ extern "C" int compute_rhs_bssn_(
   for (int f = 0; f < 6; ++f) AMSS_CK(cudaMemcpyAsync(rc[f], dR + f * fs, bytes, cudaMemcpyDeviceToHost, s));
   if (*co == 0)
     for (int f = 0; f < 7; ++f) AMSS_CK(cudaMemcpyAsync(cs[f], dc + f * fs, bytes, cudaMemcpyDeviceToHost, s));
+  AMSS_CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+extern "C" int compute_rhs_z4c_(
+    int* ex, double* T, double* X, double* Y, double* Z, double* chi, double* trK, double* dxx, double* gxy,
+    double* gxz, double* dyy, double* gyz, double* dzz, double* Axx, double* Axy, double* Axz, double* Ayy,
+    double* Ayz, double* Azz, double* Gamx, double* Gamy, double* Gamz, double* Lap, double* betax, double* betay,
+    double* betaz, double* dtSfx, double* dtSfy, double* dtSfz, double* TZ, double* chi_rhs, double* trK_rhs,
+    double* gxx_rhs, double* gxy_rhs, double* gxz_rhs, double* gyy_rhs, double* gyz_rhs, double* gzz_rhs,
+    double* Axx_rhs, double* Axy_rhs, double* Axz_rhs, double* Ayy_rhs, double* Ayz_rhs, double* Azz_rhs,
+    double* Gamx_rhs, double* Gamy_rhs, double* Gamz_rhs, double* Lap_rhs, double* betax_rhs, double* betay_rhs,
+    double* betaz_rhs, double* dtSfx_rhs, double* dtSfy_rhs, double* dtSfz_rhs, double* TZ_rhs, double* rho,
+    double* Sx, double* Sy, double* Sz, double* Sxx, double* Sxy, double* Sxz, double* Syy, double* Syz, double* Szz,
+    double* Gamxxx, double* Gamxxy, double* Gamxxz, double* Gamxyy, double* Gamxyz, double* Gamxzz, double* Gamyxx,
+    double* Gamyxy, double* Gamyxz, double* Gamyyy, double* Gamyyz, double* Gamyzz, double* Gamzxx, double* Gamzxy,
+    double* Gamzxz, double* Gamzyy, double* Gamzyz, double* Gamzzz, double* Rxx, double* Rxy, double* Rxz,
+    double* Ryy, double* Ryz, double* Rzz, double* Hcon, double* Mxcon, double* Mycon, double* Mzcon,
+    double* Gmxcon, double* Gmycon, double* Gmzcon, int* Symmetry, int* Lev, double* eps, int* co) {
+  (void)T;
+  (void)Lev;
+  (void)co;   // Z4c_rhs.f90:147: the constraints are always computed
+  if (!ex || ex[0] < 3 || ex[1] < 3 || ex[2] < 3) return amss_fail(AMSS_ERR_ARG, "compute_rhs_z4c_: every extent must be >= 3");
+  DropinCtx& c = g_ctx;
+  if (c.init() != 0) return AMSS_ERR_NO_DEVICE;
+  const long long n = (long long)ex[0] * ex[1] * ex[2];
+  const long long fs = pad_stride(n);
+  // layout: 25 state | 10 matter | 25 rhs | 24 scratch rhs | 18 gamma | 6 ricci | 7 cons | X Y Z
+  const size_t total = (size_t)fs * (25 + 10 + 25 + 24 + 18 + 6 + 7) + ex[0] + ex[1] + ex[2] + 8;
+  double* d = c.reserve(total);
+  if (!d) return amss_fail(AMSS_ERR_CUDA, "compute_rhs_z4c_: device allocation failed");
+  double* du = d;
+  double* dm = du + 25 * fs;
+  double* dr = dm + 10 * fs;
+  double* dscr = dr + 25 * fs;
+  double* dg = dscr + 24 * fs;
+  double* dR = dg + 18 * fs;
+  double* dc = dR + 6 * fs;
+  double* dX = dc + 7 * fs;
+  double* dY = dX + ex[0];
+  double* dZ = dY + ex[1];
+  double* st_in[25] = {chi, trK, dxx, gxy, gxz, dyy, gyz, dzz, Axx, Axy, Axz, Ayy, Ayz, Azz,
+                       Gamx, Gamy, Gamz, Lap, betax, betay, betaz, dtSfx, dtSfy, dtSfz, TZ};
+  double* mat[10] = {rho, Sx, Sy, Sz, Sxx, Sxy, Sxz, Syy, Syz, Szz};
+  double* rh[25] = {chi_rhs, trK_rhs, gxx_rhs, gxy_rhs, gxz_rhs, gyy_rhs, gyz_rhs, gzz_rhs,
+                    Axx_rhs, Axy_rhs, Axz_rhs, Ayy_rhs, Ayz_rhs, Azz_rhs, Gamx_rhs, Gamy_rhs, Gamz_rhs,
+                    Lap_rhs, betax_rhs, betay_rhs, betaz_rhs, dtSfx_rhs, dtSfy_rhs, dtSfz_rhs, TZ_rhs};
+  double* gm[18] = {Gamxxx, Gamxxy, Gamxxz, Gamxyy, Gamxyz, Gamxzz, Gamyxx, Gamyxy, Gamyxz,
+                    Gamyyy, Gamyyz, Gamyzz, Gamzxx, Gamzxy, Gamzxz, Gamzyy, Gamzyz, Gamzzz};
+  double* rc[6] = {Rxx, Rxy, Rxz, Ryy, Ryz, Rzz};
+  double* cs[7] = {Hcon, Mxcon, Mycon, Mzcon, Gmxcon, Gmycon, Gmzcon};
+  const size_t bytes = (size_t)n * sizeof(double);
+  cudaStream_t s = c.stream;
+  for (int f = 0; f < 25; ++f) AMSS_CK(cudaMemcpyAsync(du + f * fs, st_in[f], bytes, cudaMemcpyHostToDevice, s));
+  for (int f = 0; f < 10; ++f) AMSS_CK(cudaMemcpyAsync(dm + f * fs, mat[f], bytes, cudaMemcpyHostToDevice, s));
+  AMSS_CK(cudaMemcpyAsync(dX, X, ex[0] * sizeof(double), cudaMemcpyHostToDevice, s));
+  AMSS_CK(cudaMemcpyAsync(dY, Y, ex[1] * sizeof(double), cudaMemcpyHostToDevice, s));
+  AMSS_CK(cudaMemcpyAsync(dZ, Z, ex[2] * sizeof(double), cudaMemcpyHostToDevice, s));
+  AMSS_CK(cudaMemsetAsync(c.dstatus, 0, sizeof(unsigned), s));
+
+  BlockView b{};
+  b.ex[0] = ex[0]; b.ex[1] = ex[1]; b.ex[2] = ex[2];
+  b.fs = fs;
+  b.X = dX; b.Y = dY; b.Z = dZ;
+  b.dx[0] = X[1] - X[0]; b.dx[1] = Y[1] - Y[0]; b.dx[2] = Z[1] - Z[0];
+  b.symmetry = *Symmetry;
+  {
+    const double bb[6] = {X[0], Y[0], Z[0], X[ex[0] - 1], Y[ex[1] - 1], Z[ex[2] - 1]};
+    block_faces(ex, X, Y, Z, bb, *Symmetry, &b.face_mask, &b.lowsym_mask);
+  }
+  Coefs<double> C;
+  C.t = make_coef<double>(b.dx, *eps);
+  C.d = C.t;
+  const int grid = grid_for(n, 128);
+  // the 25 right-hand sides (Z4c_rhs.f90:126-1265)
+  if (b.lowsym_mask) AMSS_CK(launch_rhs_dropin_z4c<true>(grid, s, b, C, du, dr, dm, c.dstatus));
+  else AMSS_CK(launch_rhs_dropin_z4c<false>(grid, s, b, C, du, dr, dm, c.dstatus));
+  unsigned hs = 0;
+  AMSS_CK(cudaMemcpyAsync(&hs, c.dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  AMSS_CK(cudaStreamSynchronize(s));
+  if ((hs & ST_NAN) || ((hs & ST_PINF) && (hs & ST_NINF))) return 1;  // Z4c_rhs.f90:261, outputs untouched
+  // ricci_gamma + constraint_bssn (Z4c_rhs.f90:1266-1290): the BSSN diagnostic pass
+  // on the first 24 fields, its right-hand sides discarded
+  RhsAux aux{dg, dR, dc, dm, fs, 0};
+  if (b.lowsym_mask) AMSS_CK(launch_rhs_dropin<true>(grid, s, b, C, du, dscr, aux, c.dstatus));
+  else AMSS_CK(launch_rhs_dropin<false>(grid, s, b, C, du, dscr, aux, c.dstatus));
+  for (int f = 0; f < 25; ++f) AMSS_CK(cudaMemcpyAsync(rh[f], dr + f * fs, bytes, cudaMemcpyDeviceToHost, s));
+  for (int f = 0; f < 18; ++f) AMSS_CK(cudaMemcpyAsync(gm[f], dg + f * fs, bytes, cudaMemcpyDeviceToHost, s));
+  for (int f = 0; f < 6; ++f) AMSS_CK(cudaMemcpyAsync(rc[f], dR + f * fs, bytes, cudaMemcpyDeviceToHost, s));
+  for (int f = 0; f < 7; ++f) AMSS_CK(cudaMemcpyAsync(cs[f], dc + f * fs, bytes, cudaMemcpyDeviceToHost, s));
   AMSS_CK(cudaStreamSynchronize(s));
   return 0;
 }

@@ -58,32 +58,32 @@ __device__ __forceinline__ PointGates point_gates(const BlockView& b, int i, int
 
 // Finish one field: + lopsided (x, y, z) + KO, then hand it to the epilogue.
 // `add1` = 1 for the diagonal metric (advected as g = d + 1, bssn_rhs.f90:948-953).
-template <typename T, int F, typename P, typename E>
+// KO1: dissipate f + add1 rather than f (the Z4c diagonal metric).
+template <typename T, int F, bool KO1 = false, typename P, typename E>
 __device__ __forceinline__ void finish_field(const P& q, const Coefs<T>& C, const PointGates& g, T r, T bx, T by,
                                              T bz, T add1, E& epi) {
   if constexpr (P::kPre) {
-    // split form: the stencil pass stored the advection sum and the KO line sum
-    if (g.lop) r = r + q.template dv<T>(doff(F) + dslots(F) - 2);
-    if (g.ko) r = r + pick<T>(C).ko * q.template dv<T>(doff(F) + dslots(F) - 1);
+    // split form: the stencil pass stored advection + KO (0 where neither applies)
+    r = r + q.template dv<T>(doff(F) + dslots(F) - 1);
     epi.template put<F>(r);
-    return;
+  } else {
+    if (g.lop) {
+      r = lop_dir<T, F, 0>(q, C, r, bx, q.i, g.lo3[0], g.hi[0], add1);
+      r = lop_dir<T, F, 1>(q, C, r, by, q.j, g.lo3[1], g.hi[1], add1);
+      r = lop_dir<T, F, 2>(q, C, r, bz, q.k, g.lo3[2], g.hi[2], add1);
+    }
+    if (g.ko) {
+      using A = std::conditional_t<wide_field<F>(), double, T>;
+      const Coef<A>& c = pick<A>(C);
+      auto kx = [&](int o) { return q.template v<A, F>(o, 0, 0); };
+      auto ky = [&](int o) { return q.template v<A, F>(0, o, 0); };
+      auto kz = [&](int o) { return q.template v<A, F>(0, 0, o); };
+      const A ks = divh(ko_sum_rn<A, KO1>(kx), c.h[0]) + divh(ko_sum_rn<A, KO1>(ky), c.h[1]) +
+                   divh(ko_sum_rn<A, KO1>(kz), c.h[2]);
+      r = r + (T)(c.ko * ks);
+    }
+    epi.template put<F>(r);
   }
-  if (g.lop) {
-    r = lop_dir<T, F, 0>(q, C, r, bx, q.i, g.lo3[0], g.hi[0], add1);
-    r = lop_dir<T, F, 1>(q, C, r, by, q.j, g.lo3[1], g.hi[1], add1);
-    r = lop_dir<T, F, 2>(q, C, r, bz, q.k, g.lo3[2], g.hi[2], add1);
-  }
-  if (g.ko) {
-    using A = std::conditional_t<wide_field<F>(), double, T>;
-    const Coef<A>& c = pick<A>(C);
-    if constexpr (std::is_same_v<A, T>)
-      r = r + c.ko * (divh(ko_line<A, F, 0>(q), c.h[0]) + divh(ko_line<A, F, 1>(q), c.h[1]) +
-                      divh(ko_line<A, F, 2>(q), c.h[2]));
-    else
-      r = r + (T)(c.ko * (divh(ko_line<A, F, 0>(q), c.h[0]) + divh(ko_line<A, F, 1>(q), c.h[1]) +
-                          divh(ko_line<A, F, 2>(q), c.h[2])));
-  }
-  epi.template put<F>(r);
 }
 
 // NaN check of bssn_rhs.f90:110-138 on the point's own 21 checked values.
@@ -98,10 +98,29 @@ __device__ __forceinline__ unsigned nan_bits(const T* v, int n) {
   return s;
 }
 
-template <typename T, typename SI, bool SYMM, bool AUX, typename E, typename P>
+// Z4C: the Z4c right-hand side of Z4c_rhs.f90:126-1295 (25 fields, Theta
+// last; kappa1 = 0.02, kappa2 = 0 from cpbc.f90:5-20) instead of BSSN.
+// Epilogues with a member ham(T) receive the Hamiltonian constraint.
+template <typename E, typename = void>
+struct epi_wants_ham : std::false_type {};
+template <typename E>
+struct epi_wants_ham<E, std::void_t<decltype(&E::ham)>> : std::true_type {};
+
+// Type of the FP64 centre values of chi and alpha: double for the FP32 and
+// FP64 forms; a recording scalar type (the adjoint generator) maps to itself.
+template <typename T>
+struct wide {
+  using type = double;
+};
+template <typename T>
+using wide_t = typename wide<T>::type;
+
+template <typename T, typename SI, bool SYMM, bool AUX, bool Z4C = false, typename E, typename P>
 __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C, const PointGates& G,
                                                    const RhsAux& aux, E& epi) {
   static_assert(!(AUX && P::kPre), "the diagnostic outputs need the stencil accessor");
+  static_assert(!(AUX && Z4C), "Z4c diagnostics come from the BSSN diagnostic pass");
+  const T kappa1 = T(0.02), kappa2 = T(0);
   const T ZEO = T(0), ONE = T(1), TWO = T(2), FOUR = T(4), EIGHT = T(8), HALF = T(0.5);
   const T FF = T(0.75), eta = T(2);
   const T F1o3 = T(1.0 / 3.0), F2o3 = T(2.0 / 3.0), F3o2 = T(1.5);
@@ -110,7 +129,8 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
 
   // centre values; chi and alpha are read and shifted in FP64 (chi -> 0 near a
   // puncture, so chi+1 must be formed before rounding to T)
-  const double chi64 = q.template v<double, F_CHI>(0, 0, 0), Lap64 = q.template v<double, F_LAP>(0, 0, 0);
+  using W = wide_t<T>;
+  const W chi64 = q.template v<W, F_CHI>(0, 0, 0), Lap64 = q.template v<W, F_LAP>(0, 0, 0);
   const T chi = (T)chi64, trK = q.template v<T, F_TRK>(0, 0, 0);
   const T dxx = q.template v<T, F_GXX>(0, 0, 0), gxy = q.template v<T, F_GXY>(0, 0, 0);
   const T gxz = q.template v<T, F_GXZ>(0, 0, 0), dyy = q.template v<T, F_GYY>(0, 0, 0);
@@ -124,16 +144,24 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   const T betaz = q.template v<T, F_BETAZ>(0, 0, 0);
   const T dtSfx = q.template v<T, F_DTSFX>(0, 0, 0), dtSfy = q.template v<T, F_DTSFY>(0, 0, 0);
   const T dtSfz = q.template v<T, F_DTSFZ>(0, 0, 0);
+  T TZ = ZEO;
+  if constexpr (Z4C) TZ = q.template v<T, F_TZ>(0, 0, 0);
   unsigned status;
-  {
+  if constexpr (Z4C) {  // Z4c_rhs.f90:230-262 checks 25 fields
+    const T chk[25] = {chi, trK, dxx, gxy, gxz, dyy, gyz, dzz, Axx, Axy, Axz, Ayy, Ayz, Azz,
+                       Gamx, Gamy, Gamz, Lap, betax, betay, betaz, dtSfx, dtSfy, dtSfz, TZ};
+    status = nan_bits(chk, 25);
+  } else {
     const T chk[21] = {chi, trK, dxx, gxy, gxz, dyy, gyz, dzz, Axx, Axy, Axz, Ayy, Ayz, Azz,
                        Gamx, Gamy, Gamz, Lap, betax, betay, betaz};
     status = nan_bits(chk, 21);
   }
+  // Z4c: K + 2 Theta wherever the evolution uses the trace (Z4c_rhs.f90:277)
+  const T trKd = Z4C ? trK + TWO * TZ : trK;
 
-  // matter (zero in vacuum)
+  // matter (zero in vacuum: the engine passes no matter fields)
   T rho = ZEO, Sx = ZEO, Sy = ZEO, Sz = ZEO, Sxx = ZEO, Sxy = ZEO, Sxz = ZEO, Syy = ZEO, Syz = ZEO, Szz = ZEO;
-  if constexpr (AUX) {
+  {
     if (aux.matter) {
       const double* m = aux.matter + q.p;
       rho = (T)m[0]; Sx = (T)m[aux.fs]; Sy = (T)m[2 * aux.fs]; Sz = (T)m[3 * aux.fs];
@@ -142,7 +170,7 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
     }
   }
 
-  const T alpn1 = (T)(Lap64 + 1.0), chin1 = (T)(chi64 + 1.0);
+  const T alpn1 = (T)(Lap64 + W(1.0)), chin1 = (T)(chi64 + W(1.0));
   const T gxx = dxx + ONE, gyy = dyy + ONE, gzz = dzz + ONE;
 
   // :152-160
@@ -153,7 +181,7 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   const T div_beta = betaxx + betayy + betazz;
   T chix, chiy, chiz;
   grad<T, F_CHI>(q, C, ord, chix, chiy, chiz);
-  finish_field<T, F_CHI>(q, C, G, F2o3 * chin1 * (alpn1 * trK - div_beta), betax, betay, betaz, ZEO, epi);
+  finish_field<T, F_CHI>(q, C, G, F2o3 * chin1 * (alpn1 * trKd - div_beta), betax, betay, betaz, ZEO, epi);
 
   // :791-795 gauge pieces that need nothing else
   finish_field<T, F_LAP>(q, C, G, -TWO * alpn1 * trK, betax, betay, betaz, ZEO, epi);
@@ -170,15 +198,15 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   grad<T, F_GYZ>(q, C, ord, gyzx, gyzy, gyzz);
   grad<T, F_GZZ>(q, C, ord, gzzx, gzzy, gzzz);
 
-  finish_field<T, F_GXX>(q, C, G,
+  finish_field<T, F_GXX, Z4C>(q, C, G,
                          -TWO * alpn1 * Axx - F2o3 * gxx * div_beta +
                              TWO * (gxx * betaxx + gxy * betayx + gxz * betazx),
                          betax, betay, betaz, ONE, epi);
-  finish_field<T, F_GYY>(q, C, G,
+  finish_field<T, F_GYY, Z4C>(q, C, G,
                          -TWO * alpn1 * Ayy - F2o3 * gyy * div_beta +
                              TWO * (gxy * betaxy + gyy * betayy + gyz * betazy),
                          betax, betay, betaz, ONE, epi);
-  finish_field<T, F_GZZ>(q, C, G,
+  finish_field<T, F_GZZ, Z4C>(q, C, G,
                          -TWO * alpn1 * Azz - F2o3 * gzz * div_beta +
                              TWO * (gxz * betaxz + gyz * betayz + gzz * betazz),
                          betax, betay, betaz, ONE, epi);
@@ -265,6 +293,13 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   {
     T Kx, Ky, Kz;
     grad<T, F_TRK>(q, C, ord, Kx, Ky, Kz);
+    if constexpr (Z4C) {  // Z4c_rhs.f90:582-586: K_,i + Theta_,i / 2
+      T tx, ty, tz;
+      grad<T, F_TZ>(q, C, ord, tx, ty, tz);
+      Kx = Kx + tx / TWO;
+      Ky = Ky + ty / TWO;
+      Kz = Kz + tz / TWO;
+    }
     const T Rxx = gupxx * gupxx * Axx + gupxy * gupxy * Ayy + gupxz * gupxz * Azz +
                   TWO * (gupxx * gupxy * Axy + gupxx * gupxz * Axz + gupxy * gupxz * Ayz);
     const T Ryy = gupxy * gupxy * Axx + gupyy * gupyy * Ayy + gupyz * gupyz * Azz +
@@ -325,9 +360,16 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
                TWO * (gupxy * bz_xy + gupxz * bz_xz + gupyz * bz_yz);
   }
   // :797-799 (GAUGE 0) and the advection / dissipation of Gam^i and B^i
-  finish_field<T, F_GAMX>(q, C, G, Gamx_rhs, betax, betay, betaz, ZEO, epi);
-  finish_field<T, F_GAMY>(q, C, G, Gamy_rhs, betax, betay, betaz, ZEO, epi);
-  finish_field<T, F_GAMZ>(q, C, G, Gamz_rhs, betax, betay, betaz, ZEO, epi);
+  if constexpr (Z4C) {
+    // Z4c_rhs.f90:1231-1233 constraint damping (B^i takes the undamped source)
+    finish_field<T, F_GAMX>(q, C, G, Gamx_rhs - TWO * alpn1 * kappa1 * (Gamx - Gamxa), betax, betay, betaz, ZEO, epi);
+    finish_field<T, F_GAMY>(q, C, G, Gamy_rhs - TWO * alpn1 * kappa1 * (Gamy - Gamya), betax, betay, betaz, ZEO, epi);
+    finish_field<T, F_GAMZ>(q, C, G, Gamz_rhs - TWO * alpn1 * kappa1 * (Gamz - Gamza), betax, betay, betaz, ZEO, epi);
+  } else {
+    finish_field<T, F_GAMX>(q, C, G, Gamx_rhs, betax, betay, betaz, ZEO, epi);
+    finish_field<T, F_GAMY>(q, C, G, Gamy_rhs, betax, betay, betaz, ZEO, epi);
+    finish_field<T, F_GAMZ>(q, C, G, Gamz_rhs, betax, betay, betaz, ZEO, epi);
+  }
   finish_field<T, F_DTSFX>(q, C, G, Gamx_rhs - eta * dtSfx, betax, betay, betaz, ZEO, epi);
   finish_field<T, F_DTSFY>(q, C, G, Gamy_rhs - eta * dtSfy, betax, betay, betaz, ZEO, epi);
   finish_field<T, F_DTSFZ>(q, C, G, Gamz_rhs - eta * dtSfz, betax, betay, betaz, ZEO, epi);
@@ -557,6 +599,9 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
     Rxz = Rxz + (fxz - chix * chiz / chin1 / TWO + gxz * f) / chin1 / TWO;
     Ryz = Ryz + (fyz - chiy * chiz / chin1 / TWO + gyz * f) / chin1 / TWO;
   }
+  // Z4c_rhs.f90:913-915: R / chi, the trace of the A~_ij source and of H
+  T Hc = ZEO;
+  if constexpr (Z4C) Hc = gupxx * Rxx + gupyy * Ryy + gupzz * Rzz + TWO * (gupxy * Rxy + gupxz * Rxz + gupyz * Ryz);
 
   // :629-660 D_i D_j alpha with the physical connection
   hess<T, F_LAP>(q, C, ord, fxx, fxy, fxz, fyy, fyz, fzz);
@@ -608,34 +653,46 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   // A_ij A^ij as written at :670-694 (sum of gup^ij times the rows above)
   const T AijAij = gupxx * AAxx + gupyy * AAyy + gupzz * AAzz + TWO * (gupxy * AAxy + gupxz * AAxz + gupyz * AAyz);
   {
-    T S = chin1 * (gupxx * Sxx + gupyy * Syy + gupzz * Szz + TWO * (gupxy * Sxy + gupxz * Sxz + gupyz * Syz));
-    T f = F2o3 * trK * trK - AijAij - T(16) * PI * rho + EIGHT * PI * S;
-    f = -F1o3 * (gupxx * fxx + gupyy * fyy + gupzz * fzz + TWO * (gupxy * fxy + gupxz * fxz + gupyz * fyz) +
-                 alpn1 / chin1 * f);
-    const T axx = alpn1 * (Rxx - EIGHT * PI * Sxx) - fxx;
-    const T axy = alpn1 * (Rxy - EIGHT * PI * Sxy) - fxy;
-    const T axz = alpn1 * (Rxz - EIGHT * PI * Sxz) - fxz;
-    const T ayy = alpn1 * (Ryy - EIGHT * PI * Syy) - fyy;
-    const T ayz = alpn1 * (Ryz - EIGHT * PI * Syz) - fyz;
-    const T azz = alpn1 * (Rzz - EIGHT * PI * Szz) - fzz;
+    T S, f, axx, axy, axz, ayy, ayz, azz;
+    if constexpr (Z4C) {
+      // Z4c_rhs.f90:964-982: the trace of the source from the Ricci scalar
+      const T sxx = EIGHT * PI * alpn1 * Sxx + fxx, sxy = EIGHT * PI * alpn1 * Sxy + fxy;
+      const T sxz = EIGHT * PI * alpn1 * Sxz + fxz, syy = EIGHT * PI * alpn1 * Syy + fyy;
+      const T syz = EIGHT * PI * alpn1 * Syz + fyz, szz = EIGHT * PI * alpn1 * Szz + fzz;
+      f = gupxx * sxx + gupyy * syy + gupzz * szz + TWO * (gupxy * sxy + gupxz * sxz + gupyz * syz);
+      f = F1o3 * (Hc * alpn1 - f);
+      axx = alpn1 * Rxx - sxx; axy = alpn1 * Rxy - sxy; axz = alpn1 * Rxz - sxz;
+      ayy = alpn1 * Ryy - syy; ayz = alpn1 * Ryz - syz; azz = alpn1 * Rzz - szz;
+    } else {
+      S = chin1 * (gupxx * Sxx + gupyy * Syy + gupzz * Szz + TWO * (gupxy * Sxy + gupxz * Sxz + gupyz * Syz));
+      f = F2o3 * trK * trK - AijAij - T(16) * PI * rho + EIGHT * PI * S;
+      f = -F1o3 * (gupxx * fxx + gupyy * fyy + gupzz * fzz + TWO * (gupxy * fxy + gupxz * fxz + gupyz * fyz) +
+                   alpn1 / chin1 * f);
+      axx = alpn1 * (Rxx - EIGHT * PI * Sxx) - fxx;
+      axy = alpn1 * (Rxy - EIGHT * PI * Sxy) - fxy;
+      axz = alpn1 * (Rxz - EIGHT * PI * Sxz) - fxz;
+      ayy = alpn1 * (Ryy - EIGHT * PI * Syy) - fyy;
+      ayz = alpn1 * (Ryz - EIGHT * PI * Syz) - fyz;
+      azz = alpn1 * (Rzz - EIGHT * PI * Szz) - fzz;
+    }
     T Axx_rhs = axx - gxx * f, Ayy_rhs = ayy - gyy * f, Azz_rhs = azz - gzz * f;
     T Axy_rhs = axy - gxy * f, Axz_rhs = axz - gxz * f, Ayz_rhs = ayz - gyz * f;
     const T fc = chin1;
     trK_rhs = fc * trK_rhs;
-    Axx_rhs = fc * Axx_rhs + alpn1 * (trK * Axx - TWO * AAxx) + TWO * (Axx * betaxx + Axy * betayx + Axz * betazx) -
+    Axx_rhs = fc * Axx_rhs + alpn1 * (trKd * Axx - TWO * AAxx) + TWO * (Axx * betaxx + Axy * betayx + Axz * betazx) -
               F2o3 * Axx * div_beta;
-    Ayy_rhs = fc * Ayy_rhs + alpn1 * (trK * Ayy - TWO * AAyy) + TWO * (Axy * betaxy + Ayy * betayy + Ayz * betazy) -
+    Ayy_rhs = fc * Ayy_rhs + alpn1 * (trKd * Ayy - TWO * AAyy) + TWO * (Axy * betaxy + Ayy * betayy + Ayz * betazy) -
               F2o3 * Ayy * div_beta;
-    Azz_rhs = fc * Azz_rhs + alpn1 * (trK * Azz - TWO * AAzz) + TWO * (Axz * betaxz + Ayz * betayz + Azz * betazz) -
+    Azz_rhs = fc * Azz_rhs + alpn1 * (trKd * Azz - TWO * AAzz) + TWO * (Axz * betaxz + Ayz * betayz + Azz * betazz) -
               F2o3 * Azz * div_beta;
-    Axy_rhs = fc * Axy_rhs + alpn1 * (trK * Axy - TWO * AAxy) + Axx * betaxy + Axz * betazy + Ayy * betayx +
+    Axy_rhs = fc * Axy_rhs + alpn1 * (trKd * Axy - TWO * AAxy) + Axx * betaxy + Axz * betazy + Ayy * betayx +
               Ayz * betazx + F1o3 * Axy * div_beta - Axy * betazz;
-    Ayz_rhs = fc * Ayz_rhs + alpn1 * (trK * Ayz - TWO * AAyz) + Axy * betaxz + Ayy * betayz + Axz * betaxy +
+    Ayz_rhs = fc * Ayz_rhs + alpn1 * (trKd * Ayz - TWO * AAyz) + Axy * betaxz + Ayy * betayz + Axz * betaxy +
               Azz * betazy + F1o3 * Ayz * div_beta - Ayz * betaxx;
-    Axz_rhs = fc * Axz_rhs + alpn1 * (trK * Axz - TWO * AAxz) + Axx * betaxz + Axy * betayz + Ayz * betayx +
+    Axz_rhs = fc * Axz_rhs + alpn1 * (trKd * Axz - TWO * AAxz) + Axx * betaxz + Axy * betayz + Ayz * betayx +
               Azz * betazx + F1o3 * Axz * div_beta - Axz * betayy;
     S = fc * (gupxx * Sxx + gupyy * Syy + gupzz * Szz + TWO * (gupxy * Sxy + gupxz * Sxz + gupyz * Syz));
-    trK_rhs = -trK_rhs + alpn1 * (F1o3 * trK * trK + gupxx * AAxx + gupyy * AAyy + gupzz * AAzz +
+    trK_rhs = -trK_rhs + alpn1 * (F1o3 * trKd * trKd + gupxx * AAxx + gupyy * AAyy + gupzz * AAzz +
                                   TWO * (gupxy * AAxy + gupxz * AAxz + gupyz * AAyz) + FOUR * PI * (rho + S));
     finish_field<T, F_AXX>(q, C, G, Axx_rhs, betax, betay, betaz, ZEO, epi);
     finish_field<T, F_AXY>(q, C, G, Axy_rhs, betax, betay, betaz, ZEO, epi);
@@ -643,7 +700,23 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
     finish_field<T, F_AYY>(q, C, G, Ayy_rhs, betax, betay, betaz, ZEO, epi);
     finish_field<T, F_AYZ>(q, C, G, Ayz_rhs, betax, betay, betaz, ZEO, epi);
     finish_field<T, F_AZZ>(q, C, G, Azz_rhs, betax, betay, betaz, ZEO, epi);
-    finish_field<T, F_TRK>(q, C, G, trK_rhs, betax, betay, betaz, ZEO, epi);
+    if constexpr (Z4C) {
+      // Z4c_rhs.f90:1230 damping; :1077-1110, :1165, :1229 Theta
+      finish_field<T, F_TRK>(q, C, G, trK_rhs + alpn1 * kappa1 * (ONE - kappa2) * TZ, betax, betay, betaz, ZEO, epi);
+      const T Hcon = chin1 * Hc + F2o3 * trKd * trKd - AijAij - T(16) * PI * rho;
+      finish_field<T, F_TZ>(q, C, G, alpn1 * Hcon / TWO - alpn1 * (TWO + kappa2) * kappa1 * TZ, betax, betay, betaz,
+                            ZEO, epi);
+    } else {
+      finish_field<T, F_TRK>(q, C, G, trK_rhs, betax, betay, betaz, ZEO, epi);
+    }
+  }
+
+  // Hamiltonian constraint (bssn_rhs.f90:1047-1075, the BSSN form that
+  // constraint_bssn also evaluates) for epilogues that ask for it: the
+  // adjoint generator records it as the integrand of its loss.
+  if constexpr (epi_wants_ham<E>::value) {
+    const T h = gupxx * Rxx + gupyy * Ryy + gupzz * Rzz + TWO * (gupxy * Rxy + gupxz * Rxz + gupyz * Ryz);
+    epi.ham(chin1 * h + F2o3 * trK * trK - AijAij - T(16) * PI * rho);
   }
 
   if constexpr (AUX) {

@@ -172,6 +172,8 @@ struct StepBlock {
   long long doff;     // offset of this block's points in the level's D slots (split form)
   long long npts;
   int lev0;           // 1: Sommerfeld rule on the patch faces; 0: freeze them at u0
+  int nf;             // evolved fields: 24 (BSSN) or 25 (Z4c, Theta last)
+  int dw;             // stencil-pass tile width (deriv_tile_w of ex[0])
 };
 
 }  // namespace amss

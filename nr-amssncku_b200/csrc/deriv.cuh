@@ -1,25 +1,59 @@
 // deriv.cuh -- the stencil pass of the split RK4 substep.
 //
-// One CTA takes one field of one (x, y) tile of a block (TX x TY points) and
-// marches through z.  A ring of 7 z-planes of the tile plus a 3-cell halo sits
-// in shared memory, filled as the reference's padded copy fh of
-// symmetry_bd (fmisc.f90:877-901): cells at negative indices hold the mirrored
-// value times the field's parity, cells past the block end are never read by
-// the gated stencils and hold 0.  Each thread evaluates, for its point, the
-// same gated stencils the per-point RHS would (diff_new.f90:946-1528,
-// lopsidediff.f90:321-481, kodiss.f90:190-207) and stores them in the D slots
-// of that field (stencil.cuh: dslots/doff); the pointwise pass reads them.
+// One CTA takes one field of one (x, y) tile of a block (W x H points, one
+// thread per column, W and H per block) and marches through z.  The planes k .. k+3 of the
+// tile plus a 3-cell halo sit in a 5-slot shared-memory ring, filled as the
+// reference's padded copy fh of symmetry_bd (fmisc.f90:877-901): cells at
+// negative indices hold the mirrored value times the field's parity, cells
+// past the block end are never read by the gated stencils and hold 0.  The
+// next plane is fetched into registers while the current one is computed,
+// so each plane costs one barrier.
 //
-// Global traffic per field and point: one plane load amortised over the z
-// march (~2.1 values per point for a 32 x 8 tile) instead of ~70 stencil loads.
+// z-direction work comes from registers: each thread keeps its column
+// f(k-3 .. k+3) and the windows of its x- and y-derivatives Dx f, Dy f at
+// planes k-2 .. k+2 (4th order) and k-1 .. k+1 (2nd order), each computed
+// once, when its plane enters the window.  The mixed
+// derivatives with z are formed as Dz(Dx f) and Dz(Dy f): the reference's
+// 16-point (4-point) cross stencils of fdderivs are exactly these tensor
+// products of its 1-D stencils, so only the rounding of the coefficient
+// product differs.  x- and y-lines and the xy cross stencil read the plane.
+//
+// Per point the pass stores, for the field's kind (stencil.cuh: dslots):
+// gradient, Hessian, and one "adv" value = upwinded advection
+// (lopsidediff.f90:321-481) + eps/64 * KO line sums (kodiss.f90:190-207).
+// The formulas and gates are those of diff_new.f90:946-1528.
 #pragma once
 #include "bssn_step.cuh"
 
 namespace amss {
 
-constexpr int DTX = 32, DTY = 8;            // tile of points per CTA
-constexpr int DSX = DTX + 6, DSY = DTY + 6; // tile plus halo
-constexpr int DPLANE = DSX * DSY;
+// A tile is W x H columns (W <= DWMAX, W * H <= DTHREADS), chosen per block
+// (deriv_tile) so that narrow blocks do not leave lanes idle: W = the block's
+// x extent split into pieces of at most 64, H = DTHREADS / W rows.
+constexpr int DTHREADS = 256;
+constexpr int DWMAX = 64;
+constexpr int DPLANE = 704;                 // >= (W + 6) (H + 6) for every admissible W
+constexpr int DRING = 5;                    // resident planes: k-1 (being replaced), k .. k+3
+constexpr int DPER = (DPLANE + DTHREADS - 1) / DTHREADS;   // plane cells per thread
+
+// Tile shape of the stencil pass for a block of x extent ex0.
+__host__ __device__ constexpr int deriv_tile_w(int ex0) {
+  return (ex0 + (ex0 + DWMAX - 1) / DWMAX - 1) / ((ex0 + DWMAX - 1) / DWMAX);
+}
+__host__ __device__ constexpr int deriv_tile_h(int ex0) { return DTHREADS / deriv_tile_w(ex0); }
+constexpr int kDerivMinEx = 8;              // the split form needs blocks at least this wide in x
+constexpr bool deriv_planes_fit(int w) {
+  return w > DWMAX || ((w + 6) * (DTHREADS / w + 6) <= DPLANE && deriv_planes_fit(w + 1));
+}
+static_assert(deriv_planes_fit(kDerivMinEx), "plane buffer too small for a tile shape");
+
+// points per tile (= threads per CTA) of the staged pointwise pass (substep_staged.cuh)
+constexpr int STILE = 64;
+#ifndef AMSS_POINTWISE_STAGED   // pointwise pass of the split form: 1 staged in shared memory, 0 per-thread loads
+#define AMSS_POINTWISE_STAGED 0
+#endif
+// substep tile of the split form's pointwise pass
+constexpr int kPointwiseTile = AMSS_POINTWISE_STAGED ? STILE : 128;
 
 struct DerivItem {
   int block;   // index into the level's StepBlock table
@@ -27,146 +61,289 @@ struct DerivItem {
   int field;
 };
 
-// Shared-memory window with the interface of Pt (v / vpad).
-template <typename A>
-struct SmemPt {
-  static constexpr bool kPre = false;
-  using elem = A;
-  const A* ring;
-  int pl[7];       // plane offset of dk = -3 .. 3
-  int li, lj;      // position in the tile
-  int i, j, k;     // array indices
-  long long p;
-  template <typename T, int F>
-  __device__ __forceinline__ T v(int di, int dj, int dk) const {
-    return (T)ring[pl[dk + 3] + (lj + dj + 3) * DSX + (li + di + 3)];
+// kind of a field's stencil record: 0 gradient + Hessian + adv, 1 gradient + adv, 2 adv
+__host__ __device__ constexpr int dkind(int F) { return dslots(F) == 10 ? 0 : (dslots(F) == 4 ? 1 : 2); }
+
+__device__ __forceinline__ int ring_slot(int m) { return (m + 3) % DRING; }   // m >= -3
+
+// The plane cells one thread fills, with their in-plane offsets and the x/y
+// mirror signs, fixed for the whole march.
+template <typename A, typename S>
+struct PlaneFetch {
+  const S* src;
+  long long sz;
+  int ex2;
+  int off[DPER];     // i + j * ex0 of the (mirrored) cell, -1: none / past the end
+  unsigned neg;      // bit e: x/y mirroring flips the sign of cell e
+  bool zodd;         // field parity in z is odd
+  A v[DPER];
+
+  __device__ __forceinline__ void init(const S* s, int F, const int* ex, int x0, int y0, int sx, int np) {
+    src = s;
+    sz = (long long)ex[0] * ex[1];
+    ex2 = ex[2];
+    zodd = soa_sign(F, 2) < 0;
+    neg = 0;
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      int o = -1;
+      if (t < np) {
+        int i = x0 - 3 + t % sx, j = y0 - 3 + t / sx;
+        bool n = false;
+        if (i < 0) { i = -i - 1; n ^= soa_sign(F, 0) < 0; }
+        if (j < 0) { j = -j - 1; n ^= soa_sign(F, 1) < 0; }
+        if (i < ex[0] && j < ex[1]) o = i + j * ex[0];
+        if (n) neg |= 1u << e;
+      }
+      off[e] = o;
+    }
   }
-  template <typename T, int F>
-  __device__ __forceinline__ T vpad(int di, int dj, int dk) const {
-    return v<T, F>(di, dj, dk);
+  // issue the loads of plane kk (negative: mirrored, past the end: 0)
+  __device__ __forceinline__ void fetch(int kk) {
+    int k = kk;
+    bool nz = false;
+    if (k < 0) { k = -k - 1; nz = zodd; }
+    const bool kin = k < ex2;
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      A x = A(0);
+      if (kin && off[e] >= 0) {
+        x = (A)__ldg(src + off[e] + k * sz);
+        if ((((neg >> e) & 1u) != 0) != nz) x = -x;
+      }
+      v[e] = x;
+    }
+  }
+  __device__ __forceinline__ void store(A* slot, int np) const {
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      if (t < np) slot[t] = v[e];
+    }
   }
 };
 
-// Load plane kk of field F of the stage input into ring slot `slot`.
-template <int F, typename A, typename SI>
-__device__ __forceinline__ void load_plane(A* ring, int slot, const SI* base, const double* side, long long fs,
-                                           const int* ex, int x0, int y0, int kk) {
-  A* dst = ring + slot * DPLANE;
-  const long long sz = (long long)ex[0] * ex[1];
-  bool negk = false;
-  int k = kk;
-  if (k < 0) { k = -k - 1; negk = soa_sign(F, 2) < 0; }
-  const bool kin = k < ex[2];
-  for (int t = threadIdx.x; t < DPLANE; t += blockDim.x) {
-    const int a = t % DSX, b = t / DSX;
-    int i = x0 - 3 + a, j = y0 - 3 + b;
-    bool neg = negk;
-    if (i < 0) { i = -i - 1; neg ^= (soa_sign(F, 0) < 0); }
-    if (j < 0) { j = -j - 1; neg ^= (soa_sign(F, 1) < 0); }
-    A v = A(0);
-    if (kin && i < ex[0] && j < ex[1]) {
-      const long long o = i + (long long)j * ex[0] + k * sz;
-      if constexpr (sizeof(SI) == 4 && wide_field<F>()) v = (A)__ldg(side + side_slot(F) * fs + o);
-      else v = (A)__ldg(base + F * fs + o);
-      if (neg) v = -v;
-    }
-    dst[t] = v;
+// Upwinded term of one direction (lopsidediff.f90:321-481) over a line f(o),
+// o = -3 .. 3 relative to the point; f already includes the +1 of the
+// diagonal metric.  bd = beta * d12.
+template <typename A, typename FN>
+__device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, int hi) {
+  const A F3 = A(3), F10 = A(10), F18 = A(18), F6 = A(6), EIT = A(8);
+  A d = A(0);
+  if (b > A(0)) {
+    if (idx + 3 <= hi) d = bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
+    else if (idx + 2 <= hi) d = bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+    else if (idx + 1 <= hi) d = -bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+  } else if (b < A(0)) {
+    if (idx - 3 >= lo) d = -bd * (-F3 * f(1) - F10 * f(0) + F18 * f(-1) - F6 * f(-2) + f(-3));
+    else if (idx - 2 >= lo) d = bd * (f(-2) - EIT * f(-1) + EIT * f(1) - f(2));
+    else if (idx - 1 >= lo) d = bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
   }
+  return d;
 }
 
-template <typename T, int F, typename SI>
-__device__ __forceinline__ void deriv_field(const StepBlock<T>& B, const SI* in, const double* in_side, int x0, int y0,
-                                            T* D, long long dfs, unsigned char* smem) {
-  using A = std::conditional_t<wide_field<F>(), double, T>;   // shared-memory and stencil type
-  A* ring = reinterpret_cast<A*>(smem);
+// March one field of one tile.  A: stencil arithmetic type, S: type of the
+// field's source array, SI: type of the stage input (for the shift), T: type
+// of the D array.
+template <typename A, int KIND, typename T, typename S, typename SI>
+__device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, int F, int x0,
+                                             int y0, T* D, long long dfs, A* ring) {
   const Coef<A>& C = pick<A>(B.C);
-  const int* ex = B.b.ex;
-  const int li = threadIdx.x % DTX, lj = threadIdx.x / DTX;
+  const int ex0 = B.b.ex[0], ex1 = B.b.ex[1], ex2 = B.b.ex[2];
+  const long long fs = B.b.fs;
+  const int W = B.dw, H = DTHREADS / W;
+  const int DSX = W + 6;                     // row stride of the plane buffer
+  const int np = DSX * (H + 6);              // cells of one plane (<= DPLANE)
+  const int li = threadIdx.x % W, lj = threadIdx.x / W;
   const int i = x0 + li, j = y0 + lj;
-  const bool mine = i < ex[0] && j < ex[1];
+  const bool mine = lj < H && i < ex0 && j < ex1;
   const int fm = B.b.face_mask;
+  const bool face_xy = ((fm & 1) && i == ex0 - 1) || ((fm & 2) && j == ex1 - 1) || ((fm & 8) && i == 0) ||
+                       ((fm & 16) && j == 0);
+  // the diagonal metric is advected as g = d + 1 (bssn_rhs.f90:948-953) in FP64,
+  // bit-faithful to the reference; FP32 advects d (the constant drops out)
+  const A add1 = (sizeof(A) == 8 && (F == F_GXX || F == F_GYY || F == F_GZZ)) ? A(1) : A(0);
+  const int o = doff(F);
   T* d = D + B.doff;
-  for (int m = 0; m < 6; ++m) load_plane<F, A>(ring, m, in, in_side, B.b.fs, ex, x0, y0, m - 3);
-  for (int k = 0; k < ex[2]; ++k) {
-    load_plane<F, A>(ring, (k + 6) % 7, in, in_side, B.b.fs, ex, x0, y0, k + 3);
+  const int own = (lj < H ? lj + 3 : 3) * DSX + (li + 3);   // idle threads read a valid cell
+
+  PlaneFetch<A, S> P;
+  P.init(src, F, B.b.ex, x0, y0, DSX, np);
+
+  A c[7];                  // column f(k-3 .. k+3)
+  A fx4[5], fy4[5];        // 4th-order Dx f, Dy f at planes k-2 .. k+2 (KIND 0)
+  A fx2[3], fy2[3];        // 2nd-order Dx f, Dy f at planes k-1 .. k+1 (KIND 0)
+
+  auto dx4 = [&](const A* q) { return C.d12[0] * (q[-2] - A(8) * q[-1] + A(8) * q[1] - q[2]); };
+  auto dy4 = [&](const A* q) { return C.d12[1] * (q[-2 * DSX] - A(8) * q[-DSX] + A(8) * q[DSX] - q[2 * DSX]); };
+  auto dx2 = [&](const A* q) { return C.d2[0] * (-q[-1] + q[1]); };
+  auto dy2 = [&](const A* q) { return C.d2[1] * (-q[-DSX] + q[DSX]); };
+
+  // prologue: planes -3 .. 3 one at a time; the column gets -3 .. 3 and the
+  // derivative windows planes -2 .. 1
+#pragma unroll 1
+  for (int m = -3; m <= 3; ++m) {
+    P.fetch(m);
+    A* slot = ring + ring_slot(m) * DPLANE;
+    P.store(slot, np);
     __syncthreads();
-    const bool on_face = ((fm & 1) && i == ex[0] - 1) || ((fm & 2) && j == ex[1] - 1) ||
-                         ((fm & 4) && k == ex[2] - 1) || ((fm & 8) && i == 0) || ((fm & 16) && j == 0) ||
-                         ((fm & 32) && k == 0);
-    if (mine && !on_face) {
-      SmemPt<A> q;
-      q.ring = ring;
-      for (int m = 0; m < 7; ++m) q.pl[m] = ((k + m) % 7) * DPLANE;
-      q.li = li;
-      q.lj = lj;
-      q.i = i;
-      q.j = j;
-      q.k = k;
-      q.p = i + (long long)j * ex[0] + (long long)k * ex[0] * ex[1];
-      const PointGates G = point_gates(B.b, i, j, k);
-      constexpr int ns = dslots(F);
-      constexpr int o = doff(F);
-      const long long pp = q.p;
-      if constexpr (ns == 11) {
-        A fx, fy, fz, fxx, fxy, fxz, fyy, fyz, fzz;
-        grad_a<A, F>(q, C, G.ord, fx, fy, fz);
-        hess_a<A, F>(q, C, G.ord, fxx, fxy, fxz, fyy, fyz, fzz);
-        d[(o + 0) * dfs + pp] = (T)fx; d[(o + 1) * dfs + pp] = (T)fy; d[(o + 2) * dfs + pp] = (T)fz;
-        d[(o + 3) * dfs + pp] = (T)fxx; d[(o + 4) * dfs + pp] = (T)fxy; d[(o + 5) * dfs + pp] = (T)fxz;
-        d[(o + 6) * dfs + pp] = (T)fyy; d[(o + 7) * dfs + pp] = (T)fyz; d[(o + 8) * dfs + pp] = (T)fzz;
-      } else if constexpr (ns == 5) {
-        A fx, fy, fz;
-        grad_a<A, F>(q, C, G.ord, fx, fy, fz);
-        d[(o + 0) * dfs + pp] = (T)fx; d[(o + 1) * dfs + pp] = (T)fy; d[(o + 2) * dfs + pp] = (T)fz;
+    const A* q = slot + own;
+    const A cm = q[0];
+#pragma unroll
+    for (int t = 0; t < 7; ++t)
+      if (t == m + 3) c[t] = cm;
+    if constexpr (KIND == 0) {
+      if (m >= -2 && m <= 1) {
+        const A a4 = dx4(q), b4 = dy4(q), a2 = dx2(q), b2 = dy2(q);
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if (t == m + 2) { fx4[t] = a4; fy4[t] = b4; }
+#pragma unroll
+        for (int t = 0; t < 2; ++t)
+          if (t == m + 1) { fx2[t] = a2; fy2[t] = b2; }
       }
-      // advection: beta at the point from the input (the shift is never a wide field)
-      const long long cp = q.p;
-      const T bx = (T)__ldg(in + F_BETAX * B.b.fs + cp);
-      const T by = (T)__ldg(in + F_BETAY * B.b.fs + cp);
-      const T bz = (T)__ldg(in + F_BETAZ * B.b.fs + cp);
-      const A add1 = (F == F_GXX || F == F_GYY || F == F_GZZ) ? A(1) : A(0);
-      A lop = A(0);
-      if (G.lop) {
-        Coefs<A> CC;
-        CC.t = C;
-        CC.d = pick<double>(B.C);
-        lop = lop_dir<A, F, 0>(q, CC, lop, (A)bx, i, G.lo3[0], G.hi[0], add1);
-        lop = lop_dir<A, F, 1>(q, CC, lop, (A)by, j, G.lo3[1], G.hi[1], add1);
-        lop = lop_dir<A, F, 2>(q, CC, lop, (A)bz, k, G.lo3[2], G.hi[2], add1);
-      }
-      A ko = A(0);
-      if (G.ko)
-        ko = divh(ko_line<A, F, 0>(q), C.h[0]) + divh(ko_line<A, F, 1>(q), C.h[1]) + divh(ko_line<A, F, 2>(q), C.h[2]);
-      d[(o + ns - 2) * dfs + pp] = (T)lop;
-      d[(o + ns - 1) * dfs + pp] = (T)ko;
     }
+  }
+
+#pragma unroll 1
+  for (int k = 0; k < ex2; ++k) {
+    P.fetch(k + 4);   // in flight while plane k is computed
+    const A* qk = ring + ring_slot(k) * DPLANE + own;
+    c[6] = ring[ring_slot(k + 3) * DPLANE + own];
+    if constexpr (KIND == 0) {
+      const A* q2 = ring + ring_slot(k + 2) * DPLANE + own;
+      const A* q1 = ring + ring_slot(k + 1) * DPLANE + own;
+      fx4[4] = dx4(q2); fy4[4] = dy4(q2); fx2[2] = dx2(q1); fy2[2] = dy2(q1);
+    }
+    const bool on_face = face_xy || ((fm & 4) && k == ex2 - 1) || ((fm & 32) && k == 0);
+    if (mine && !on_face) {
+      const PointGates G = point_gates(B.b, i, j, k);
+      const long long p = i + (long long)j * ex0 + (long long)k * ex0 * ex1;
+      auto X = [&](int dd) { return qk[dd]; };
+      auto Y = [&](int dd) { return qk[dd * DSX]; };
+      auto Z = [&](int dd) { return c[3 + dd]; };
+      if constexpr (KIND <= 1) {
+        A gx = A(0), gy = A(0), gz = A(0);
+        if (G.ord == 2) {
+          if constexpr (KIND == 0) { gx = fx4[2]; gy = fy4[2]; }
+          else { gx = dx4(qk); gy = dy4(qk); }
+          gz = C.d12[2] * (Z(-2) - A(8) * Z(-1) + A(8) * Z(1) - Z(2));
+        } else if (G.ord == 1) {
+          if constexpr (KIND == 0) { gx = fx2[1]; gy = fy2[1]; }
+          else { gx = dx2(qk); gy = dy2(qk); }
+          gz = C.d2[2] * (-Z(-1) + Z(1));
+        }
+        d[(o + 0) * dfs + p] = (T)gx;
+        d[(o + 1) * dfs + p] = (T)gy;
+        d[(o + 2) * dfs + p] = (T)gz;
+      }
+      if constexpr (KIND == 0) {
+        A hxx = A(0), hxy = A(0), hxz = A(0), hyy = A(0), hyz = A(0), hzz = A(0);
+        const A F16 = A(16), F30 = A(30), F8 = A(8), TWO = A(2);
+        if (G.ord == 2) {
+          hxx = C.Fdd[0] * (-X(-2) + F16 * X(-1) - F30 * X(0) - X(2) + F16 * X(1));
+          hyy = C.Fdd[1] * (-Y(-2) + F16 * Y(-1) - F30 * Y(0) - Y(2) + F16 * Y(1));
+          hzz = C.Fdd[2] * (-Z(-2) + F16 * Z(-1) - F30 * Z(0) - Z(2) + F16 * Z(1));
+          auto row = [&](int ob) {
+            const A* r = qk + ob * DSX;
+            return r[-2] - F8 * r[-1] + F8 * r[1] - r[2];
+          };
+          hxy = C.Fxy * (row(-2) - F8 * row(-1) + F8 * row(1) - row(2));
+          hxz = C.d12[2] * (fx4[0] - F8 * fx4[1] + F8 * fx4[3] - fx4[4]);
+          hyz = C.d12[2] * (fy4[0] - F8 * fy4[1] + F8 * fy4[3] - fy4[4]);
+        } else if (G.ord == 1) {
+          hxx = C.Sdd[0] * (X(-1) - TWO * X(0) + X(1));
+          hyy = C.Sdd[1] * (Y(-1) - TWO * Y(0) + Y(1));
+          hzz = C.Sdd[2] * (Z(-1) - TWO * Z(0) + Z(1));
+          hxy = C.Sxy * (qk[-1 - DSX] - qk[1 - DSX] - qk[-1 + DSX] + qk[1 + DSX]);
+          hxz = C.d2[2] * (-fx2[0] + fx2[2]);
+          hyz = C.d2[2] * (-fy2[0] + fy2[2]);
+        }
+        d[(o + 3) * dfs + p] = (T)hxx;
+        d[(o + 4) * dfs + p] = (T)hxy;
+        d[(o + 5) * dfs + p] = (T)hxz;
+        d[(o + 6) * dfs + p] = (T)hyy;
+        d[(o + 7) * dfs + p] = (T)hyz;
+        d[(o + 8) * dfs + p] = (T)hzz;
+      }
+      A adv = A(0);
+      if (G.lop) {
+        // the shift at the point, from the stage input (never a wide field)
+        const T bx = (T)__ldg(in + F_BETAX * fs + p);
+        const T by = (T)__ldg(in + F_BETAY * fs + p);
+        const T bz = (T)__ldg(in + F_BETAZ * fs + p);
+        auto Xp = [&](int dd) { return X(dd) + add1; };
+        auto Yp = [&](int dd) { return Y(dd) + add1; };
+        auto Zp = [&](int dd) { return Z(dd) + add1; };
+        adv = lop_term<A>(Xp, (A)bx, (A)bx * C.d12[0], i, G.lo3[0], G.hi[0]);
+        adv = adv + lop_term<A>(Yp, (A)by, (A)by * C.d12[1], j, G.lo3[1], G.hi[1]);
+        adv = adv + lop_term<A>(Zp, (A)bz, (A)bz * C.d12[2], k, G.lo3[2], G.hi[2]);
+      }
+      if (G.ko) {
+        // Z4c dissipates the full diagonal metric d + 1 (Z4c_rhs.f90:1240-1245)
+        const bool ko1 = B.nf == NFIELDS_Z4C && (F == F_GXX || F == F_GYY || F == F_GZZ);
+        A ks;
+        if (ko1)
+          ks = divh(ko_sum_rn<A, true>(X), C.h[0]) + divh(ko_sum_rn<A, true>(Y), C.h[1]) +
+               divh(ko_sum_rn<A, true>(Z), C.h[2]);
+        else
+          ks = divh(ko_sum_rn<A, false>(X), C.h[0]) + divh(ko_sum_rn<A, false>(Y), C.h[1]) +
+               divh(ko_sum_rn<A, false>(Z), C.h[2]);
+        adv = adv + C.ko * ks;
+      }
+      d[(o + dslots(F) - 1) * dfs + p] = (T)adv;
+    }
+    // slide the register windows
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c[t] = c[t + 1];
+    if constexpr (KIND == 0) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) { fx4[t] = fx4[t + 1]; fy4[t] = fy4[t + 1]; }
+#pragma unroll
+      for (int t = 0; t < 2; ++t) { fx2[t] = fx2[t + 1]; fy2[t] = fy2[t + 1]; }
+    }
+    // plane k+4 replaces plane k-1, which no thread reads in this iteration
+    P.store(ring + ring_slot(k + 4) * DPLANE, np);
     __syncthreads();
   }
 }
 
-// Stencil pass over a work list of (block, tile, field) items.
+// Stencil pass over a work list of (block, tile, field) items, ordered by
+// field so that resident CTAs share one code path.
 template <typename T, typename SI>
-__global__ void __launch_bounds__(DTX * DTY) k_deriv(const StepBlock<T>* __restrict__ blocks,
-                                                     const DerivItem* __restrict__ items, int nitems, int sub,
-                                                     T* __restrict__ D, long long dfs) {
+__global__ void __launch_bounds__(DTHREADS, 2) k_deriv(const StepBlock<T>* __restrict__ blocks,
+                                                      const DerivItem* __restrict__ items, int nitems, int sub,
+                                                      T* __restrict__ D, long long dfs) {
   extern __shared__ __align__(16) unsigned char smem[];
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const DerivItem it = items[w];
     const StepBlock<T>& B = blocks[it.block];
     const int cur = B.lvl[0];
     const SI* in = sub == 0 ? (const SI*)B.tl[cur] : (const SI*)B.stage[sub == 2 ? 1 : 0];
-    const double* in_side = sub == 0 ? nullptr : B.side[sub == 2 ? 1 : 0];
-    switch (it.field) {
-#define AMSS_DF(F) case F: deriv_field<T, F, SI>(B, in, in_side, it.x0, it.y0, D, dfs, smem); break;
-      AMSS_DF(F_CHI) AMSS_DF(F_TRK) AMSS_DF(F_GXX) AMSS_DF(F_GXY) AMSS_DF(F_GXZ) AMSS_DF(F_GYY)
-      AMSS_DF(F_GYZ) AMSS_DF(F_GZZ) AMSS_DF(F_AXX) AMSS_DF(F_AXY) AMSS_DF(F_AXZ) AMSS_DF(F_AYY)
-      AMSS_DF(F_AYZ) AMSS_DF(F_AZZ) AMSS_DF(F_GAMX) AMSS_DF(F_GAMY) AMSS_DF(F_GAMZ) AMSS_DF(F_LAP)
-      AMSS_DF(F_BETAX) AMSS_DF(F_BETAY) AMSS_DF(F_BETAZ) AMSS_DF(F_DTSFX) AMSS_DF(F_DTSFY) AMSS_DF(F_DTSFZ)
-#undef AMSS_DF
-      default: break;
+    const int F = it.field;
+    const long long fs = B.b.fs;
+    if constexpr (sizeof(T) == 4) {
+      if (F == F_CHI || F == F_LAP) {
+        // wide fields of the mixed form: FP64 source (state, or the FP64 side stage) and arithmetic
+        const double* src = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F) * fs
+                                            : (const double*)in + F * fs;
+        deriv_column<double, 0>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<double*>(smem));
+        __syncthreads();
+        continue;
+      }
+    }
+    const SI* src = in + F * fs;
+    switch (dkind(F)) {
+      case 0: deriv_column<T, 0>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 1: deriv_column<T, 1>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      default: deriv_column<T, 2>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
     }
     __syncthreads();
   }
 }
+
+// Shared memory of k_deriv: the plane ring in the widest arithmetic type.
+constexpr size_t kDerivSmem = (size_t)DRING * DPLANE * sizeof(double);
 
 }  // namespace amss

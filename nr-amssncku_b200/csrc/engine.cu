@@ -31,9 +31,12 @@ template <typename T>
 Coef<T> make_coef(const double dx[3], double eps);
 void block_faces(const int ex[3], const double* X, const double* Y, const double* Z, const double bbox[6],
                  int symmetry, int* face_mask, int* lowsym_mask);
-template <typename T, typename SS, bool SYMM, bool SPLIT>
+template <typename T, typename SS, bool SYMM, bool SPLIT, bool Z4C>
 cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, int sub, RKConst rk, int enforce,
                            unsigned* status, int grid, cudaStream_t s, const void* D, long long dfs);
+template <typename T, typename SS, bool SYMM>
+cudaError_t launch_face(const void* blocks, const int2* faces, int nfaces, int sub, RKConst rk, int enforce,
+                        unsigned* status, cudaStream_t s);
 template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
                          int grid, cudaStream_t s);
@@ -136,6 +139,8 @@ struct ELevel {
   DevBoxes sync, restrict_, prolong;
   int2* dti_tiles = nullptr;    // time-interpolation tiles (global block ids)
   int nti = 0;
+  int2* dfaces = nullptr;       // outer-face points (table index, point) for k_face
+  int nfaces = 0;
   DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
   int nditems = 0;
   long long dfs = 0;            // slot stride of D for this level
@@ -166,6 +171,7 @@ struct amss_engine {
   long long launches = 0;
   bool committed = false;
   int sm_count = 148;
+  int nf = NFIELDS_BSSN;        // evolved fields: 24 (BSSN) or 25 (Z4c)
 };
 
 extern "C" const char* amss_last_error(void) { return g_err.c_str(); }
@@ -174,8 +180,17 @@ extern "C" const char* amss_version(void) { return "amss_b200 0.2 (sm_100a)"; }
 extern "C" amss_engine* amss_engine_create(const amss_params* prm) {
   if (!prm) { amss_fail(AMSS_ERR_ARG, "amss_engine_create: null params"); return nullptr; }
   if (check_device("amss_engine_create") != 0) return nullptr;
+  if (prm->formulation != 0 && prm->formulation != 1) {
+    amss_fail(AMSS_ERR_ARG, "amss_engine_create: formulation must be 0 (BSSN) or 1 (Z4c)");
+    return nullptr;
+  }
+  if (prm->formulation == 1 && prm->kernel != 0) {
+    amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_create: Z4c runs the split kernel form only");
+    return nullptr;
+  }
   amss_engine* e = new amss_engine();
   e->prm = *prm;
+  e->nf = prm->formulation == 1 ? NFIELDS_Z4C : NFIELDS_BSSN;
   if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&e->dstatus, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(e->dstatus, 0, sizeof(unsigned)) != cudaSuccess) {
@@ -198,6 +213,7 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.dtable) cudaFree(L.dtable);
     if (L.dti_tiles) cudaFree(L.dti_tiles);
     if (L.ditems) cudaFree(L.ditems);
+    if (L.dfaces) cudaFree(L.dfaces);
     L.sync.release();
     L.restrict_.release();
     L.prolong.release();
@@ -227,7 +243,8 @@ static void finish_block(amss_engine* e, EBlock& b, const double bbox[6], const 
 extern "C" int amss_engine_add_block(amss_engine* e, int level, const int ex[3], const double bbox[6],
                                      const double patch_bbox[6]) {
   if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_add_block: engine already committed");
-  if (ex[0] < 7 || ex[1] < 7 || ex[2] < 7) return amss_fail(AMSS_ERR_ARG, "amss_engine_add_block: ex < 7");
+  if (ex[0] < kDerivMinEx || ex[1] < 7 || ex[2] < 7)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_add_block: needs ex[0] >= 8 and ex[1], ex[2] >= 7");
   EBlock b;
   b.level = level;
   for (int d = 0; d < 3; ++d) {
@@ -266,6 +283,8 @@ extern "C" int amss_engine_add_amr_block(amss_engine* e, int level, int patch, c
   if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_add_amr_block: engine already committed");
   if (!e->grid_set) return amss_fail(AMSS_ERR_STATE, "amss_engine_add_amr_block: call amss_engine_set_grid first");
   if (level < 0 || level > 30 || buffer < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_add_amr_block: bad level/buffer");
+  if (ex[0] < kDerivMinEx || ex[1] < 7 || ex[2] < 7)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_add_amr_block: needs ex[0] >= 8 and ex[1], ex[2] >= 7");
   EBlock b;
   b.level = level;
   for (int d = 0; d < 3; ++d) {
@@ -312,6 +331,7 @@ template <typename T>
 static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<StepBlock<T>> tab;
   std::vector<int2> tiles;
+  std::vector<int2> faces;
   std::vector<DerivItem> items;
   long long doff = 0;
   for (size_t m = 0; m < L.blocks.size(); ++m) {
@@ -319,9 +339,9 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     StepBlock<T> s{};
     s.doff = doff;
     doff += b.fs;
-    for (int y0 = 0; y0 < b.ex[1]; y0 += DTY)
-      for (int x0 = 0; x0 < b.ex[0]; x0 += DTX)
-        for (int f = 0; f < 24; ++f) items.push_back(DerivItem{(int)m, x0, y0, f});
+    const int tw = deriv_tile_w(b.ex[0]), th = deriv_tile_h(b.ex[0]);
+    for (int y0 = 0; y0 < b.ex[1]; y0 += th)
+      for (int x0 = 0; x0 < b.ex[0]; x0 += tw) items.push_back(DerivItem{(int)m, x0, y0, 0});
     s.b.ex[0] = b.ex[0]; s.b.ex[1] = b.ex[1]; s.b.ex[2] = b.ex[2];
     s.b.fs = b.fs;
     s.b.X = b.dX; s.b.Y = b.dX + b.ex[0]; s.b.Z = b.dX + b.ex[0] + b.ex[1];
@@ -341,9 +361,41 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     s.K = b.K;
     s.npts = b.npts;
     s.lev0 = level == 0 ? 1 : 0;
+    s.nf = e->nf;
+    s.dw = deriv_tile_w(b.ex[0]);
     if (b.lowsym) L.symm = true;
     tab.push_back(s);
-    for (long long p = 0; p < b.npts; p += 128) tiles.push_back(make_int2((int)m, (int)p));
+    // substep tiles: kPointwiseTile points for the split form's pointwise pass, 128 for the fused kernel
+    const long long tstep = e->prm.kernel == 0 ? kPointwiseTile : 128;
+    for (long long p = 0; p < b.npts; p += tstep) tiles.push_back(make_int2((int)m, (int)p));
+    if (b.face_mask) {
+      const int fm = b.face_mask;
+      for (int k = 0; k < b.ex[2]; ++k)
+        for (int j = 0; j < b.ex[1]; ++j)
+          for (int i = 0; i < b.ex[0]; ++i) {
+            const bool on = ((fm & 1) && i == b.ex[0] - 1) || ((fm & 2) && j == b.ex[1] - 1) ||
+                            ((fm & 4) && k == b.ex[2] - 1) || ((fm & 8) && i == 0) || ((fm & 16) && j == 0) ||
+                            ((fm & 32) && k == 0);
+            if (on) faces.push_back(make_int2((int)m, (int)(i + (long long)j * b.ex[0] + (long long)k * b.ex[0] * b.ex[1])));
+          }
+    }
+  }
+  {
+    // one item per (field, tile), field-major and grouped by stencil kind
+    // (the FP64 fields of the mixed form first), so resident CTAs of the
+    // stencil pass run the same code
+    static const int order[25] = {F_CHI, F_LAP, F_BETAX, F_BETAY, F_BETAZ, F_GXX, F_GXY, F_GXZ,
+                                  F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
+                                  F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
+    std::vector<DerivItem> tiles_only;
+    tiles_only.swap(items);
+    for (int f : order) {
+      if (f == F_TZ && e->nf != NFIELDS_Z4C) continue;
+      for (DerivItem it : tiles_only) {
+        it.field = f;
+        items.push_back(it);
+      }
+    }
   }
   L.ntiles = (int)tiles.size();
   L.dfs = doff;
@@ -352,6 +404,11 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   AMSS_CK(cudaMalloc(&L.dtable, tab.size() * sizeof(StepBlock<T>)));
   AMSS_CK(cudaMemcpy(L.dtable, tab.data(), tab.size() * sizeof(StepBlock<T>), cudaMemcpyHostToDevice));
+  L.nfaces = (int)faces.size();
+  if (!faces.empty()) {
+    AMSS_CK(cudaMalloc(&L.dfaces, faces.size() * sizeof(int2)));
+    AMSS_CK(cudaMemcpy(L.dfaces, faces.data(), faces.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
   AMSS_CK(cudaMalloc(&L.dtiles, tiles.size() * sizeof(int2)));
   AMSS_CK(cudaMemcpy(L.dtiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
   return 0;
@@ -459,8 +516,8 @@ extern "C" int amss_engine_commit(amss_engine* e) {
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
   for (auto& b : e->blocks) {
     bytes += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
-    bytes += align((size_t)24 * b.fs * sizeof(double)) * 4;  // 3 time levels + K
-    bytes += align((size_t)24 * b.fs * ss) * 2;              // two stages
+    bytes += align((size_t)e->nf * b.fs * sizeof(double)) * 4;  // 3 time levels + K
+    bytes += align((size_t)e->nf * b.fs * ss) * 2;              // two stages
     if (mixed) bytes += align((size_t)2 * b.fs * sizeof(double)) * 2;
   }
   AMSS_CK(cudaMalloc(&e->arena, bytes));
@@ -470,10 +527,10 @@ extern "C" int amss_engine_commit(amss_engine* e) {
   for (auto& b : e->blocks) {
     b.dX = (double*)p;
     p += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
-    for (int t = 0; t < 3; ++t) { b.tl[t] = (double*)p; p += align((size_t)24 * b.fs * sizeof(double)); }
-    b.K = (double*)p; p += align((size_t)24 * b.fs * sizeof(double));
-    b.st[0] = p; p += align((size_t)24 * b.fs * ss);
-    b.st[1] = p; p += align((size_t)24 * b.fs * ss);
+    for (int t = 0; t < 3; ++t) { b.tl[t] = (double*)p; p += align((size_t)e->nf * b.fs * sizeof(double)); }
+    b.K = (double*)p; p += align((size_t)e->nf * b.fs * sizeof(double));
+    b.st[0] = p; p += align((size_t)e->nf * b.fs * ss);
+    b.st[1] = p; p += align((size_t)e->nf * b.fs * ss);
     if (mixed) {
       b.side[0] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
       b.side[1] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
@@ -495,6 +552,7 @@ extern "C" int amss_engine_commit(amss_engine* e) {
     a.side[0] = b.side[0]; a.side[1] = b.side[1];
     a.K = b.K;
     a.lvl = e->dlvl + 2 * b.level;
+    a.nf = e->nf;
   }
   AMSS_CK(cudaMalloc(&e->dblocks, ab.size() * sizeof(AmrBlock)));
   AMSS_CK(cudaMemcpy(e->dblocks, ab.data(), ab.size() * sizeof(AmrBlock), cudaMemcpyHostToDevice));
@@ -518,7 +576,8 @@ extern "C" int amss_engine_commit(amss_engine* e) {
   if (e->prm.kernel == 0) {
     long long mx = 0;
     for (auto& kv : e->levels) mx = std::max(mx, kv.second.dfs);
-    AMSS_CK(cudaMalloc(&e->D, (size_t)mx * D_SLOTS * (mixed ? sizeof(float) : sizeof(double))));
+    const int slots = e->nf == NFIELDS_Z4C ? D_SLOTS_Z4C : D_SLOTS;
+    AMSS_CK(cudaMalloc(&e->D, (size_t)mx * slots * (mixed ? sizeof(float) : sizeof(double))));
   }
   e->committed = true;
   return 0;
@@ -536,7 +595,7 @@ extern "C" int amss_engine_set_state(amss_engine* e, int block, const double* h)
   if (int rc = check_block(e, block)) return rc;
   EBlock& b = e->blocks[block];
   AMSS_CK(cudaMemcpy2DAsync(cur_state(e, b), b.fs * sizeof(double), h, b.npts * sizeof(double),
-                            b.npts * sizeof(double), 24, cudaMemcpyHostToDevice, e->stream));
+                            b.npts * sizeof(double), e->nf, cudaMemcpyHostToDevice, e->stream));
   AMSS_CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -545,7 +604,7 @@ extern "C" int amss_engine_get_state(amss_engine* e, int block, double* h) {
   if (int rc = check_block(e, block)) return rc;
   EBlock& b = e->blocks[block];
   AMSS_CK(cudaMemcpy2DAsync(h, b.npts * sizeof(double), cur_state(e, b), b.fs * sizeof(double),
-                            b.npts * sizeof(double), 24, cudaMemcpyDeviceToHost, e->stream));
+                            b.npts * sizeof(double), e->nf, cudaMemcpyDeviceToHost, e->stream));
   AMSS_CK(cudaStreamSynchronize(e->stream));
   return 0;
 }
@@ -604,17 +663,29 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
       AMSS_CK(ed);
       e->launches++;
     }
-#define AMSS_SUB(T, SY, SP) \
-    launch_substep<T, T, SY, SP>(L.dtable, L.dtiles, L.ntiles, sub, rk, enf, e->dstatus, grid, e->stream, e->D, L.dfs)
-    if (mixed)
-      err = split ? (L.symm ? AMSS_SUB(float, true, true) : AMSS_SUB(float, false, true))
-                  : (L.symm ? AMSS_SUB(float, true, false) : AMSS_SUB(float, false, false));
+#define AMSS_SUB(T, SY, SP, Z) \
+    launch_substep<T, T, SY, SP, Z>(L.dtable, L.dtiles, L.ntiles, sub, rk, enf, e->dstatus, grid, e->stream, e->D, L.dfs)
+    if (e->nf == NFIELDS_Z4C)   // split form only (checked at create)
+      err = mixed ? (L.symm ? AMSS_SUB(float, true, true, true) : AMSS_SUB(float, false, true, true))
+                  : (L.symm ? AMSS_SUB(double, true, true, true) : AMSS_SUB(double, false, true, true));
+    else if (mixed)
+      err = split ? (L.symm ? AMSS_SUB(float, true, true, false) : AMSS_SUB(float, false, true, false))
+                  : (L.symm ? AMSS_SUB(float, true, false, false) : AMSS_SUB(float, false, false, false));
     else
-      err = split ? (L.symm ? AMSS_SUB(double, true, true) : AMSS_SUB(double, false, true))
-                  : (L.symm ? AMSS_SUB(double, true, false) : AMSS_SUB(double, false, false));
+      err = split ? (L.symm ? AMSS_SUB(double, true, true, false) : AMSS_SUB(double, false, true, false))
+                  : (L.symm ? AMSS_SUB(double, true, false, false) : AMSS_SUB(double, false, false, false));
 #undef AMSS_SUB
     AMSS_CK(err);
     e->launches++;
+    if (L.nfaces) {
+      const cudaError_t ef =
+          mixed ? (L.symm ? launch_face<float, float, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
+                          : launch_face<float, float, false>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream))
+                : (L.symm ? launch_face<double, double, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
+                          : launch_face<double, double, false>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream));
+      AMSS_CK(ef);
+      e->launches++;
+    }
     if (sub < 3) {
       if (int rc = sync_level(e, L, sub == 1 ? BUF_STAGE_B : BUF_STAGE_A)) return rc;
     }
@@ -738,6 +809,7 @@ extern "C" int amss_engine_sync(amss_engine* e) {
   unsigned st = 0;
   AMSS_CK(cudaMemcpy(&st, e->dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (st & ST_BAD_ARG) return amss_fail(AMSS_ERR_STATE, "a kernel met a box outside its block (engine tables)");
+  if (st & ST_TIMEOUT) return amss_fail(AMSS_ERR_CUDA, "a bounded wait on an asynchronous copy gave up");
   return ((st & ST_NAN) || ((st & ST_PINF) && (st & ST_NINF))) ? 1 : 0;
 }
 

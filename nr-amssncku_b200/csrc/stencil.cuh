@@ -97,22 +97,25 @@ struct Pt {
 
 // ---- precomputed stencil terms (split form) ----------------------------------
 // The stencil pass (deriv.cuh) stores, per point and field, what the RHS needs
-// of that field's neighbourhood: gradient (3), Hessian (6: xx xy xz yy yz zz),
-// the summed upwinded advection and the summed KO line sums -- 11 values for
-// the shift, chi, the metric and the lapse, 5 for trK and Gamma^i (gradient,
-// advection, KO), 2 for A~ij and B^i (advection, KO): 159 slots in all.
+// of that field's neighbourhood: gradient (3), Hessian (6: xx xy xz yy yz zz)
+// and "adv" = upwinded advection + eps/64 * KO line sums -- 10 values for the
+// shift, chi, the metric and the lapse, 4 for trK and Gamma^i (gradient, adv),
+// 1 for A~ij and B^i (adv): 135 slots in all (Z4c: + 4 for Theta).
 __host__ __device__ constexpr int dslots(int F) {
   return (F == F_BETAX || F == F_BETAY || F == F_BETAZ || F == F_CHI || F == F_LAP || (F >= F_GXX && F <= F_GZZ))
-             ? 11
-             : ((F == F_TRK || F == F_GAMX || F == F_GAMY || F == F_GAMZ) ? 5 : 2);
+             ? 10
+             : ((F == F_TRK || F == F_GAMX || F == F_GAMY || F == F_GAMZ || F == F_TZ) ? 4 : 1);
 }
 __host__ __device__ constexpr int doff(int F) {
   int o = 0;
   for (int f = 0; f < F; ++f) o += dslots(f);
   return o;
 }
-constexpr int D_SLOTS = 159;
+constexpr int D_SLOTS = 135;
 static_assert(doff(24) == D_SLOTS, "D slot layout");
+// Z4c: Theta's gradient and adv follow (slots 135-138)
+constexpr int D_SLOTS_Z4C = D_SLOTS + 4;
+static_assert(doff(F_TZ) == D_SLOTS && doff(F_TZ + 1) == D_SLOTS_Z4C, "Z4c D slot layout");
 
 // Accessor of the pointwise pass: centre values from the stage input (Pt),
 // stencil terms from the D array written by the stencil pass.
@@ -161,12 +164,12 @@ template <typename T, int F, typename P>
 __device__ __forceinline__ void grad(const P& q, const Coefs<T>& C, int ord, T& fx, T& fy, T& fz) {
   if constexpr (P::kPre) {
     fx = q.template dv<T>(doff(F) + 0); fy = q.template dv<T>(doff(F) + 1); fz = q.template dv<T>(doff(F) + 2);
-    return;
+  } else {
+    using A = std::conditional_t<wide_field<F>(), double, T>;
+    A ax, ay, az;
+    grad_a<A, F>(q, pick<A>(C), ord, ax, ay, az);
+    fx = (T)ax; fy = (T)ay; fz = (T)az;
   }
-  using A = std::conditional_t<wide_field<F>(), double, T>;
-  A ax, ay, az;
-  grad_a<A, F>(q, pick<A>(C), ord, ax, ay, az);
-  fx = (T)ax; fy = (T)ay; fz = (T)az;
 }
 
 // ---- second derivatives (fdderivs) ------------------------------------------
@@ -230,12 +233,12 @@ __device__ __forceinline__ void hess(const P& q, const Coefs<T>& C, int ord, T& 
     const int o = doff(F) + 3;
     fxx = q.template dv<T>(o); fxy = q.template dv<T>(o + 1); fxz = q.template dv<T>(o + 2);
     fyy = q.template dv<T>(o + 3); fyz = q.template dv<T>(o + 4); fzz = q.template dv<T>(o + 5);
-    return;
+  } else {
+    using A = std::conditional_t<wide_field<F>(), double, T>;
+    A a[6];
+    hess_a<A, F>(q, pick<A>(C), ord, a[0], a[1], a[2], a[3], a[4], a[5]);
+    fxx = (T)a[0]; fxy = (T)a[1]; fxz = (T)a[2]; fyy = (T)a[3]; fyz = (T)a[4]; fzz = (T)a[5];
   }
-  using A = std::conditional_t<wide_field<F>(), double, T>;
-  A a[6];
-  hess_a<A, F>(q, pick<A>(C), ord, a[0], a[1], a[2], a[3], a[4], a[5]);
-  fxx = (T)a[0]; fxy = (T)a[1]; fxz = (T)a[2]; fyy = (T)a[3]; fyz = (T)a[4]; fzz = (T)a[5];
 }
 
 // ---- upwinded advection (lopsided), one direction ---------------------------
@@ -248,7 +251,10 @@ __device__ __forceinline__ T lop_dir(const P& q, const Coefs<T>& CC, T r, T b, i
   const Coef<A>& C = pick<A>(CC);
   const A F3 = A(3), F10 = A(10), F18 = A(18), F6 = A(6), EIT = A(8);
   auto f = [&](int o) -> A {
-    return q.template vpad<A, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)) + A(add1);
+    // FP32: the stencil of the offset d, not of d + 1 (the weights sum to zero,
+    // and 1 + d in FP32 keeps only ~6e-8 of d)
+    if constexpr (sizeof(A) == 4) return q.template vpad<A, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2));
+    else return q.template vpad<A, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)) + A(add1);
   };
   const A bd = A(b) * C.d12[D];
   if constexpr (std::is_same_v<A, T>) {
@@ -289,6 +295,29 @@ __device__ __forceinline__ T ko_line(const P& q) {
   const T SIX = T(6), FIT = T(15), TWT = T(20);
   auto f = [&](int o) -> T { return q.template v<T, F>(o * ax<D>(0), o * ax<D>(1), o * ax<D>(2)); };
   return (f(-3) + f(3)) - SIX * (f(-2) + f(2)) + FIT * (f(-1) + f(1)) - TWT * f(0);
+}
+
+// The same line sum in FP64 with every operation rounded as written (no
+// contraction into FMA), i.e. as the Fortran evaluates it.  ADD1: sum f + 1,
+// where the reference dissipates the full diagonal metric g = d + 1
+// (Z4c_rhs.f90:1240-1245).  A KO term acting on O(1e-8)
+// noise in an O(1) field is a difference of O(1) values, so any other
+// rounding differs from the reference's in relative terms far above 1e-12.
+template <typename T, bool ADD1, typename FN>
+__device__ __forceinline__ T ko_sum_rn(const FN& f) {
+  // FP32: always the sum of d (KO annihilates the constant; 1 + d in FP32 keeps ~6e-8 of d)
+  if constexpr (sizeof(T) == 8) {
+    auto g = [&](int o) {
+      if constexpr (ADD1) return __dadd_rn(f(o), 1.0);
+      else return (double)f(o);
+    };
+    double s = __dadd_rn(g(-3), g(3));
+    s = __dsub_rn(s, __dmul_rn(6.0, __dadd_rn(g(-2), g(2))));
+    s = __dadd_rn(s, __dmul_rn(15.0, __dadd_rn(g(-1), g(1))));
+    return __dsub_rn(s, __dmul_rn(20.0, g(0)));
+  } else {
+    return (f(-3) + f(3)) - T(6) * (f(-2) + f(2)) + T(15) * (f(-1) + f(1)) - T(20) * f(0);
+  }
 }
 
 template <typename T>

@@ -3,6 +3,6 @@
 #include "substep_impl.cuh"
 
 namespace amss {
-template cudaError_t launch_substep<float, float, true, true>(const void*, const int2*, int, int, RKConst, int,
+template cudaError_t launch_substep<float, float, true, true, false>(const void*, const int2*, int, int, RKConst, int,
                                                        unsigned*, int, cudaStream_t, const void*, long long);
 }  // namespace amss

@@ -2,46 +2,53 @@
 // Instantiated in one translation unit per (precision, symmetry) pair so the
 // large kernels compile in parallel.
 #pragma once
-#include "deriv.cuh"
+#include "substep_staged.cuh"
+
+#ifndef AMSS_SUBSTEP_MINB   // resident CTAs of 128 threads the register-pass kernel is compiled for
+#define AMSS_SUBSTEP_MINB 2
+#endif
+#ifndef AMSS_POINTWISE_PREFETCH   // L2 prefetch of the next tile's rows in the register pass
+#define AMSS_POINTWISE_PREFETCH 0
+#endif
 
 namespace amss {
-
-__device__ __forceinline__ void point_ijk(long long p, const int* ex, int& i, int& j, int& k) {
-  const long long s1 = (long long)ex[0] * ex[1];
-  k = (int)(p / s1);
-  const long long r = p - (long long)k * s1;
-  j = (int)(r / ex[0]);
-  i = (int)(r - (long long)j * ex[0]);
-}
-
-template <typename SI, bool SYMM>
-__device__ __forceinline__ Pt<SI, SYMM> make_pt(const SI* base, const BlockView& b, long long p,
-                                               const double* side = nullptr) {
-  Pt<SI, SYMM> q;
-  q.base = base;
-  q.side = side;
-  q.fs = b.fs;
-  q.p = p;
-  q.sy = b.ex[0];
-  q.sz = (long long)b.ex[0] * b.ex[1];
-  point_ijk(p, b.ex, q.i, q.j, q.k);
-  q.ex0 = b.ex[0];
-  q.ex1 = b.ex[1];
-  q.ex2 = b.ex[2];
-  return q;
-}
 
 // Fused RK4 substep over a tile list of one level.  Substep `sub` reads
 // (sub0: u0, sub1: A, sub2: B, sub3: A) and writes (A, B, A, unew).
 // SPLIT: the stencil terms come from the D array the stencil pass (k_deriv)
 // wrote for this substep; otherwise every stencil is evaluated here.
-template <typename T, typename SI, typename SO, bool SYMM, bool SPLIT>
-__global__ void __launch_bounds__(128) k_substep(const StepBlock<T>* __restrict__ blocks, const int2* __restrict__ tiles,
-                                                 int ntiles, int sub, RKConst rk, int enforce, unsigned* status,
-                                                 const T* __restrict__ D, long long dfs) {
+template <typename T, typename SI, typename SO, bool SYMM, bool SPLIT, bool Z4C>
+__global__ void __launch_bounds__(128, AMSS_SUBSTEP_MINB) k_substep(const StepBlock<T>* __restrict__ blocks,
+                                                                    const int2* __restrict__ tiles, int ntiles,
+                                                                    int sub, RKConst rk, int enforce,
+                                                                    unsigned* status, const T* __restrict__ D,
+                                                                    long long dfs) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
     const StepBlock<T>& B = blocks[tile.x];
+#if AMSS_POINTWISE_PREFETCH
+    // split form: pull the rows of this CTA's next tile (D slots, stage
+    // input, u0, K) into L2 while this tile computes, so its loads meet L2
+    // rather than HBM latency
+    if constexpr (SPLIT) {
+      if (threadIdx.x < 32 && t + (int)gridDim.x < ntiles) {
+        const int2 nt = tiles[t + gridDim.x];
+        const StepBlock<T>& N = blocks[nt.x];
+        const long long fs = N.b.fs, q0 = nt.y;
+        const int cur = N.lvl[0];
+        const SI* nin = sub == 0 ? (const SI*)N.tl[cur] : (const SI*)N.stage[sub == 2 ? 1 : 0];
+        for (int r = threadIdx.x; r < D_SLOTS + 72; r += 32) {
+          const void* a;
+          unsigned bytes;
+          if (r < D_SLOTS) { a = D + N.doff + r * dfs + q0; bytes = 128 * sizeof(T); }
+          else if (r < D_SLOTS + 24) { a = nin + (r - D_SLOTS) * fs + q0; bytes = 128 * sizeof(SI); }
+          else if (r < D_SLOTS + 48) { a = N.tl[cur] + (r - D_SLOTS - 24) * fs + q0; bytes = 128 * sizeof(double); }
+          else { a = N.K + (r - D_SLOTS - 48) * fs + q0; bytes = 128 * sizeof(double); }
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+        }
+      }
+    }
+#endif
     const long long p = (long long)tile.y + threadIdx.x;
     if (p >= B.npts) continue;
     const int cur = B.lvl[0];
@@ -65,78 +72,97 @@ __global__ void __launch_bounds__(128) k_substep(const StepBlock<T>* __restrict_
     const bool on_face = ((fm & 1) && q.i == q.ex0 - 1) || ((fm & 2) && q.j == q.ex1 - 1) ||
                          ((fm & 4) && q.k == q.ex2 - 1) || ((fm & 8) && q.i == 0) || ((fm & 16) && q.j == 0) ||
                          ((fm & 32) && q.k == 0);
-    unsigned st = 0;
-    if (!on_face) {
-      const PointGates G = point_gates(B.b, q.i, q.j, q.k);
-      RhsAux aux{};
-      if constexpr (SPLIT) {
-        DPt<SI, SYMM, T> qd;
-        static_cast<Pt<SI, SYMM>&>(qd) = q;
-        qd.d = D + B.doff;
-        qd.dfs = dfs;
-        st = bssn_rhs_point<T, SI, SYMM, false>(qd, B.C, G, aux, epi);
-      } else {
-        st = bssn_rhs_point<T, SI, SYMM, false>(q, B.C, G, aux, epi);
-      }
+    // outer-face points are updated by k_face (a separate list), so no warp
+    // here carries the Sommerfeld path for a few of its lanes
+    if (on_face) continue;
+    unsigned st;
+    const PointGates G = point_gates(B.b, q.i, q.j, q.k);
+    RhsAux aux{};
+    if constexpr (SPLIT) {
+      DPt<SI, SYMM, T> qd;
+      static_cast<Pt<SI, SYMM>&>(qd) = q;
+      qd.d = D + B.doff;
+      qd.dfs = dfs;
+      st = bssn_rhs_point<T, SI, SYMM, false, Z4C>(qd, B.C, G, aux, epi);
     } else {
-      // NaN check of the input, as the full RHS would do it
-      T chk[21];
-      chk[0] = q.template v<T, F_CHI>(0, 0, 0); chk[1] = q.template v<T, F_TRK>(0, 0, 0);
-      chk[2] = q.template v<T, F_GXX>(0, 0, 0); chk[3] = q.template v<T, F_GXY>(0, 0, 0);
-      chk[4] = q.template v<T, F_GXZ>(0, 0, 0); chk[5] = q.template v<T, F_GYY>(0, 0, 0);
-      chk[6] = q.template v<T, F_GYZ>(0, 0, 0); chk[7] = q.template v<T, F_GZZ>(0, 0, 0);
-      chk[8] = q.template v<T, F_AXX>(0, 0, 0); chk[9] = q.template v<T, F_AXY>(0, 0, 0);
-      chk[10] = q.template v<T, F_AXZ>(0, 0, 0); chk[11] = q.template v<T, F_AYY>(0, 0, 0);
-      chk[12] = q.template v<T, F_AYZ>(0, 0, 0); chk[13] = q.template v<T, F_AZZ>(0, 0, 0);
-      chk[14] = q.template v<T, F_GAMX>(0, 0, 0); chk[15] = q.template v<T, F_GAMY>(0, 0, 0);
-      chk[16] = q.template v<T, F_GAMZ>(0, 0, 0); chk[17] = q.template v<T, F_LAP>(0, 0, 0);
-      chk[18] = q.template v<T, F_BETAX>(0, 0, 0); chk[19] = q.template v<T, F_BETAY>(0, 0, 0);
-      chk[20] = q.template v<T, F_BETAZ>(0, 0, 0);
-      st = nan_bits(chk, 21);
-      if (B.lev0) {
-        const T x = (T)B.b.X[q.i], y = (T)B.b.Y[q.j], z = (T)B.b.Z[q.k];
-        int lo[3], hi[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          lo[d] = ((B.b.lowsym_mask >> d) & 1) ? -1 : 0;
-          hi[d] = B.b.ex[d] - 1;
-        }
-        const T v2 = T(1.4142135623730951), v1 = T(1);
-#define AMSS_SOMM(F, V) epi.template put<F>(sommerfeld_point<T, F>(q, B.d2s, lo, hi, x, y, z, V));
-        AMSS_SOMM(F_CHI, v2) AMSS_SOMM(F_TRK, v2) AMSS_SOMM(F_GXX, v1) AMSS_SOMM(F_GXY, v1)
-        AMSS_SOMM(F_GXZ, v1) AMSS_SOMM(F_GYY, v1) AMSS_SOMM(F_GYZ, v1) AMSS_SOMM(F_GZZ, v1)
-        AMSS_SOMM(F_AXX, v1) AMSS_SOMM(F_AXY, v1) AMSS_SOMM(F_AXZ, v1) AMSS_SOMM(F_AYY, v1)
-        AMSS_SOMM(F_AYZ, v1) AMSS_SOMM(F_AZZ, v1) AMSS_SOMM(F_GAMX, v1) AMSS_SOMM(F_GAMY, v1)
-        AMSS_SOMM(F_GAMZ, v1) AMSS_SOMM(F_LAP, v2) AMSS_SOMM(F_BETAX, v1) AMSS_SOMM(F_BETAY, v1)
-        AMSS_SOMM(F_BETAZ, v1) AMSS_SOMM(F_DTSFX, v1) AMSS_SOMM(F_DTSFY, v1) AMSS_SOMM(F_DTSFZ, v1)
-#undef AMSS_SOMM
-      } else {
-        epi.freeze = true;
-#define AMSS_FRZ(F) epi.template put<F>(T(0));
-        AMSS_FRZ(F_CHI) AMSS_FRZ(F_TRK) AMSS_FRZ(F_GXX) AMSS_FRZ(F_GXY) AMSS_FRZ(F_GXZ) AMSS_FRZ(F_GYY)
-        AMSS_FRZ(F_GYZ) AMSS_FRZ(F_GZZ) AMSS_FRZ(F_AXX) AMSS_FRZ(F_AXY) AMSS_FRZ(F_AXZ) AMSS_FRZ(F_AYY)
-        AMSS_FRZ(F_AYZ) AMSS_FRZ(F_AZZ) AMSS_FRZ(F_GAMX) AMSS_FRZ(F_GAMY) AMSS_FRZ(F_GAMZ) AMSS_FRZ(F_LAP)
-        AMSS_FRZ(F_BETAX) AMSS_FRZ(F_BETAY) AMSS_FRZ(F_BETAZ) AMSS_FRZ(F_DTSFX) AMSS_FRZ(F_DTSFY)
-        AMSS_FRZ(F_DTSFZ)
-#undef AMSS_FRZ
-      }
-      epi.finish();
+      st = bssn_rhs_point<T, SI, SYMM, false, Z4C>(q, B.C, G, aux, epi);
     }
     if (st) atomicOr(status, st);
   }
 }
 
-template <typename T, typename SS, bool SYMM, bool SPLIT>
+// Outer-face points of a level (Sommerfeld on level 0, frozen on refined patch
+// faces), one thread each, from the list faces[] = (block, point).
+template <typename T, typename SI, typename SO, bool SYMM>
+__global__ void __launch_bounds__(128) k_face(const StepBlock<T>* __restrict__ blocks, const int2* __restrict__ faces,
+                                              int nfaces, int sub, RKConst rk, int enforce, unsigned* status) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfaces; t += gridDim.x * blockDim.x) {
+    const int2 fc = faces[t];
+    const StepBlock<T>& B = blocks[fc.x];
+    const long long p = fc.y;
+    const int cur = B.lvl[0];
+    double* u0 = B.tl[cur];
+    const SI* in = sub == 0 ? (const SI*)u0 : (const SI*)B.stage[sub == 2 ? 1 : 0];
+    auto q = make_pt<SI, SYMM>(in, B.b, p, sub == 0 ? nullptr : B.side[sub == 2 ? 1 : 0]);
+    EpiRK<T, SO> epi;
+    epi.out_side = sub == 3 ? nullptr : B.side[sub == 1 ? 1 : 0];
+    epi.u0 = u0;
+    epi.K = B.K;
+    epi.out = sub == 3 ? (SO*)B.tl[(cur + 1) % 3] : (SO*)B.stage[sub == 1 ? 1 : 0];
+    epi.fs = B.b.fs;
+    epi.p = p;
+    epi.sub = sub;
+    epi.enforce = enforce != 0;
+    epi.c = rk;
+    epi.freeze = false;
+    const unsigned st = face_point<T, SI, SO, SYMM>(B, q, epi);
+    if (st) atomicOr(status, st);
+  }
+}
+
+template <typename T, typename SS, bool SYMM>
+cudaError_t launch_face(const void* blocks, const int2* faces, int nfaces, int sub, RKConst rk, int enforce,
+                        unsigned* status, cudaStream_t s) {
+  if (nfaces == 0) return cudaSuccess;
+  const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
+  const int grid = (nfaces + 127) / 128 < 148 * 8 ? (nfaces + 127) / 128 : 148 * 8;
+  if (sub == 0)
+    k_face<T, double, SS, SYMM><<<grid, 128, 0, s>>>(bl, faces, nfaces, sub, rk, enforce, status);
+  else if (sub == 3)
+    k_face<T, SS, double, SYMM><<<grid, 128, 0, s>>>(bl, faces, nfaces, sub, rk, enforce, status);
+  else
+    k_face<T, SS, SS, SYMM><<<grid, 128, 0, s>>>(bl, faces, nfaces, sub, rk, enforce, status);
+  return cudaGetLastError();
+}
+
+// SPLIT: the pointwise pass -- staged through shared memory over
+// STILE-point tiles when AMSS_POINTWISE_STAGED, else per-thread loads over
+// 128-point tiles (kPointwiseTile); otherwise the fused kernel (128-point tiles).
+template <typename T, typename SS, bool SYMM, bool SPLIT, bool Z4C>
 cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, int sub, RKConst rk, int enforce,
                            unsigned* status, int grid, cudaStream_t s, const void* D, long long dfs) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
   const T* d = (const T*)D;
-  if (sub == 0)
-    k_substep<T, double, SS, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
-  else if (sub == 3)
-    k_substep<T, SS, double, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
-  else
-    k_substep<T, SS, SS, SYMM, SPLIT><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  if constexpr (SPLIT && AMSS_POINTWISE_STAGED && !Z4C) {
+#define AMSS_STAGED(SI, SO)                                                                          \
+    {                                                                                                \
+      constexpr size_t sm = staged_smem_bytes<T, SI>();                                              \
+      cudaFuncSetAttribute(k_substep_staged<T, SI, SO, SYMM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                           (int)sm);                                                                 \
+      k_substep_staged<T, SI, SO, SYMM><<<grid, STILE, sm, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs); \
+    }
+    if (sub == 0) AMSS_STAGED(double, SS)
+    else if (sub == 3) AMSS_STAGED(SS, double)
+    else AMSS_STAGED(SS, SS)
+#undef AMSS_STAGED
+  } else {
+    if (sub == 0)
+      k_substep<T, double, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+    else if (sub == 3)
+      k_substep<T, SS, double, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+    else
+      k_substep<T, SS, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  }
   return cudaGetLastError();
 }
 
@@ -145,14 +171,11 @@ template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
                          int grid, cudaStream_t s) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
-  const size_t smem = 7 * DPLANE * sizeof(double);
-  if (sub == 0) {
-    cudaFuncSetAttribute(k_deriv<T, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_deriv<T, double><<<grid, DTX * DTY, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
-  } else {
-    cudaFuncSetAttribute(k_deriv<T, SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_deriv<T, SS><<<grid, DTX * DTY, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
-  }
+  const size_t smem = kDerivSmem;   // < 48 KB: no opt-in attribute needed
+  if (sub == 0)
+    k_deriv<T, double><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  else
+    k_deriv<T, SS><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
   return cudaGetLastError();
 }
 
@@ -174,6 +197,33 @@ template <bool SYMM>
 cudaError_t launch_rhs_dropin(int grid, cudaStream_t s, BlockView b, Coefs<double> C, const double* u, double* rhs,
                               RhsAux aux, unsigned* status) {
   k_rhs_dropin<SYMM><<<grid, 128, 0, s>>>(b, C, u, rhs, aux, status);
+  return cudaGetLastError();
+}
+
+// Drop-in Z4c RHS: all points of one block, the 25 right-hand sides (the
+// diagnostic outputs come from k_rhs_dropin, as ricci_gamma + constraint_bssn
+// evaluate the BSSN formulas).
+template <bool SYMM>
+__global__ void __launch_bounds__(128) k_rhs_dropin_z4c(BlockView b, Coefs<double> C, const double* __restrict__ u,
+                                                        double* __restrict__ rhs, const double* matter,
+                                                        unsigned* status) {
+  const long long n = (long long)b.ex[0] * b.ex[1] * b.ex[2];
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    auto q = make_pt<double, SYMM>(u, b, p);
+    const PointGates G = point_gates(b, q.i, q.j, q.k);
+    EpiStore<double> epi{rhs, b.fs, p};
+    RhsAux aux{};
+    aux.matter = matter;
+    aux.fs = b.fs;
+    const unsigned st = bssn_rhs_point<double, double, SYMM, false, true>(q, C, G, aux, epi);
+    if (st) atomicOr(status, st);
+  }
+}
+
+template <bool SYMM>
+cudaError_t launch_rhs_dropin_z4c(int grid, cudaStream_t s, BlockView b, Coefs<double> C, const double* u,
+                                  double* rhs, const double* matter, unsigned* status) {
+  k_rhs_dropin_z4c<SYMM><<<grid, 128, 0, s>>>(b, C, u, rhs, matter, status);
   return cudaGetLastError();
 }
 

@@ -25,7 +25,7 @@ def _p(a):
 
 
 def _ptrs(arr):
-    return (_DP * 24)(*[_p(arr[f]) for f in range(24)])
+    return (_DP * arr.shape[0])(*[_p(arr[f]) for f in range(arr.shape[0])])
 
 
 def _isect(alo, ahi, blo, bhi):
@@ -35,16 +35,18 @@ def _isect(alo, ahi, blo, bhi):
 
 
 class OracleHierarchy:
-    def __init__(self, H, eps=0.1, chitiny=1e-5 - 1.0, symmetry=0):
+    def __init__(self, H, eps=0.1, chitiny=1e-5 - 1.0, symmetry=0, nf=24):
+        """nf = 25: the Z4c evolution (Theta as the 25th field)."""
         self.H = H
+        self.nf = nf
         self.eps = eps
         self.chitiny = chitiny
         self.symmetry = symmetry
         lib = O.lib()
-        lib.oracle_bssn_substep.restype = ctypes.c_int
+        lib.oracle_evolve_substep.restype = ctypes.c_int
         self.blk = []
         for b in H.blocks:
-            shape = (24, b.ex[2], b.ex[1], b.ex[0])
+            shape = (nf, b.ex[2], b.ex[1], b.ex[0])
             X, Y, Z = H.coords(b)
             p = H.levels[b.level][b.patch]
             self.blk.append(dict(
@@ -98,11 +100,11 @@ class OracleHierarchy:
                 u0 = d["U"][c]
                 src = {0: u0, 1: d["A"], 2: d["B"], 3: d["A"]}[sub]
                 out = {0: d["A"], 1: d["B"], 2: d["A"], 3: d["U"][(c + 1) % 3]}[sub]
-                err |= lib.oracle_bssn_substep(d["ex"], _p(d["X"]), _p(d["Y"]), _p(d["Z"]), _p(d["pbbox"]),
-                                               _ptrs(u0), _ptrs(src), _ptrs(out), _ptrs(d["K"]), ctypes.c_int(sub),
-                                               ctypes.c_double(dt), ctypes.c_double(self.eps),
-                                               ctypes.c_double(self.chitiny), ctypes.c_int(self.symmetry),
-                                               ctypes.c_int(level))
+                err |= lib.oracle_evolve_substep(d["ex"], _p(d["X"]), _p(d["Y"]), _p(d["Z"]), _p(d["pbbox"]),
+                                                 _ptrs(u0), _ptrs(src), _ptrs(out), _ptrs(d["K"]), ctypes.c_int(sub),
+                                                 ctypes.c_double(dt), ctypes.c_double(self.eps),
+                                                 ctypes.c_double(self.chitiny), ctypes.c_int(self.symmetry),
+                                                 ctypes.c_int(level), ctypes.c_int(self.nf))
             if sub < 3:
                 self.sync(level, "A" if sub != 1 else "B")
         self.cur[level] = (c + 1) % 3
@@ -141,7 +143,7 @@ class OracleHierarchy:
                         continue
                     carr = self._arr(cb, ctarget)
                     farr = self.state(fb)
-                    for f in range(24):
+                    for f in range(self.nf):
                         lib.oracle_restrict3_box(_I3(*bc.ex), _I3(*bc.org), _p(carr[f]), _I3(*bf.ex), _I3(*bf.org),
                                                  _p(farr[f]), _I3(*rr[0]), _I3(*rr[1]))
         self.sync(cl, ctarget)
@@ -170,7 +172,7 @@ class OracleHierarchy:
                             continue
                         carr = self._arr(cb, ctarget)
                         farr = self.state(fb)
-                        for f in range(24):
+                        for f in range(self.nf):
                             lib.oracle_prolong3_box(_I3(*bc.ex), _I3(*bc.org), _p(carr[f]), _I3(*bf.ex),
                                                     _I3(*bf.org), _p(farr[f]), _I3(*rr[0]), _I3(*rr[1]))
         self.sync(level, "state")
@@ -209,18 +211,21 @@ def grid_noise(level, field, gi, gj, gk, seed):
     return (z >> np.uint64(11)).astype(np.float64) * (2.0 / 2.0 ** 53) - 1.0
 
 
-def initial_state(H, masses, positions, noise=0.0, seed=1):
+def initial_state(H, masses, positions, noise=0.0, seed=1, nf=24):
     """Brill-Lindquist data on every block (get_lousto_nbhs), plus uniform noise
-    of amplitude `noise` that depends only on the global cell (grid_noise)."""
+    of amplitude `noise` that depends only on the global cell (grid_noise).
+    nf = 25 appends the Z4c Theta field (zero, plus the same kind of noise)."""
     out = []
     with np.errstate(over="ignore"):
         for b in H.blocks:
             X, Y, Z = H.coords(b)
             st = O.brill_lindquist(X, Y, Z, masses, positions)
+            if nf == 25:
+                st = np.concatenate([st, np.zeros((1,) + st.shape[1:])])
             if noise > 0:
                 gk, gj, gi = np.meshgrid(np.arange(b.ex[2]) + b.org[2], np.arange(b.ex[1]) + b.org[1],
                                          np.arange(b.ex[0]) + b.org[0], indexing="ij")
-                for f in range(24):
+                for f in range(nf):
                     st[f] += noise * grid_noise(b.level, f, gi, gj, gk, seed)
             out.append(st)
     return out

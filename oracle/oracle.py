@@ -137,6 +137,28 @@ def fdderivs(X, Y, Z, f, soa=(1.0, 1.0, 1.0), symmetry=0):
     return out
 
 
+def lopsided(X, Y, Z, f, beta, soa=(1.0, 1.0, 1.0), symmetry=0):
+    """lopsidediff.f90:186-488 added to a zero right-hand side: the upwinded
+    advection beta^i d_i f."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    r = np.zeros_like(f)
+    b = [np.ascontiguousarray(x, dtype=np.float64) for x in beta]
+    s = np.ascontiguousarray(soa, dtype=np.float64)
+    lib().oracle_lopsided(_ex(f.shape), _p(X), _p(Y), _p(Z), _p(f), _p(r), _p(b[0]), _p(b[1]), _p(b[2]),
+                          ctypes.c_int(symmetry), _p(s))
+    return r
+
+
+def kodis(X, Y, Z, f, soa=(1.0, 1.0, 1.0), symmetry=0, eps=0.1):
+    """kodiss.f90:120-216 added to a zero right-hand side."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    r = np.zeros_like(f)
+    s = np.ascontiguousarray(soa, dtype=np.float64)
+    lib().oracle_kodis(_ex(f.shape), _p(X), _p(Y), _p(Z), _p(f), _p(r), _p(s), ctypes.c_int(symmetry),
+                       ctypes.c_double(eps))
+    return r
+
+
 def enforce_ga(state):
     """In place on state[2:14] (enforce_algebra.f90:72-133)."""
     ex = _ex(state.shape[1:])

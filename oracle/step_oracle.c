@@ -364,14 +364,51 @@ void oracle_average2(long n, const double *f1, const double *f2, const double *f
 /* Parity (SoA) and Sommerfeld speed of the 24 BSSN state fields in state order,
  * bssn_class.C:177-330 (parities) and :390-410 (speed sqrt(2) for chi, trK,
  * Lap; var.C:30 default 1). */
-static const double BSSN_SOA[24][3] = {
+static const double BSSN_SOA[25][3] = {
     {1, 1, 1}, {1, 1, 1}, {1, 1, 1}, {-1, -1, 1}, {-1, 1, -1}, {1, 1, 1}, {1, -1, -1}, {1, 1, 1},
     {1, 1, 1}, {-1, -1, 1}, {-1, 1, -1}, {1, 1, 1}, {1, -1, -1}, {1, 1, 1},
     {-1, 1, 1}, {1, -1, 1}, {1, 1, -1}, {1, 1, 1}, {-1, 1, 1}, {1, -1, 1}, {1, 1, -1},
-    {-1, 1, 1}, {1, -1, 1}, {1, 1, -1}};
+    {-1, 1, 1}, {1, -1, 1}, {1, 1, -1},
+    {1, 1, 1}};   /* Z4c Theta (Z4c_class.C var table: SSS, propspeed 1) */
 
 const double *oracle_bssn_soa(int field) { return BSSN_SOA[field]; }
 double oracle_bssn_propspeed(int field) { return (field == 0 || field == 1 || field == 17) ? sqrt(2.0) : 1.0; }
+
+int oracle_compute_rhs_z4c(
+    const int *ex, double T, const double *X, const double *Y, const double *Z,
+    double *chi, double *trK, double *dxx, double *gxy, double *gxz, double *dyy, double *gyz, double *dzz,
+    double *Axx, double *Axy, double *Axz, double *Ayy, double *Ayz, double *Azz,
+    double *Gamx, double *Gamy, double *Gamz,
+    double *Lap, double *betax, double *betay, double *betaz,
+    double *dtSfx, double *dtSfy, double *dtSfz, double *TZ,
+    double *chi_rhs, double *trK_rhs,
+    double *gxx_rhs, double *gxy_rhs, double *gxz_rhs, double *gyy_rhs, double *gyz_rhs, double *gzz_rhs,
+    double *Axx_rhs, double *Axy_rhs, double *Axz_rhs, double *Ayy_rhs, double *Ayz_rhs, double *Azz_rhs,
+    double *Gamx_rhs, double *Gamy_rhs, double *Gamz_rhs,
+    double *Lap_rhs, double *betax_rhs, double *betay_rhs, double *betaz_rhs,
+    double *dtSfx_rhs, double *dtSfy_rhs, double *dtSfz_rhs, double *TZ_rhs,
+    const double *rho, const double *Sx, const double *Sy, const double *Sz,
+    const double *Sxx, const double *Sxy, const double *Sxz, const double *Syy, const double *Syz, const double *Szz,
+    double *Gamxxx, double *Gamxxy, double *Gamxxz, double *Gamxyy, double *Gamxyz, double *Gamxzz,
+    double *Gamyxx, double *Gamyxy, double *Gamyxz, double *Gamyyy, double *Gamyyz, double *Gamyzz,
+    double *Gamzxx, double *Gamzxy, double *Gamzxz, double *Gamzyy, double *Gamzyz, double *Gamzzz,
+    double *Rxx, double *Rxy, double *Rxz, double *Ryy, double *Ryz, double *Rzz,
+    double *ham_Res, double *movx_Res, double *movy_Res, double *movz_Res,
+    double *Gmx_Res, double *Gmy_Res, double *Gmz_Res,
+    int Symmetry, int Lev, double eps, int co);
+
+/* Z4c rhs call on 25-pointer lists (Z4c_class.C:207, :575) */
+static int rhs_call_z4c(const int *ex, double T, const double *X, const double *Y, const double *Z, double **u,
+                        double **r, double **s, const double *zero, int Symmetry, int lev, double eps, double **c)
+{
+    return oracle_compute_rhs_z4c(
+        ex, T, X, Y, Z, u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9], u[10], u[11], u[12], u[13],
+        u[14], u[15], u[16], u[17], u[18], u[19], u[20], u[21], u[22], u[23], u[24], r[0], r[1], r[2], r[3], r[4],
+        r[5], r[6], r[7], r[8], r[9], r[10], r[11], r[12], r[13], r[14], r[15], r[16], r[17], r[18], r[19], r[20],
+        r[21], r[22], r[23], r[24], zero, zero, zero, zero, zero, zero, zero, zero, zero, zero, s[0], s[1], s[2],
+        s[3], s[4], s[5], s[6], s[7], s[8], s[9], s[10], s[11], s[12], s[13], s[14], s[15], s[16], s[17], s[18],
+        s[19], s[20], s[21], s[22], s[23], c[0], c[1], c[2], c[3], c[4], c[5], c[6], Symmetry, lev, eps, 0);
+}
 
 /* rhs call on 24-pointer state / rhs lists with vacuum matter and scratch outputs */
 static int rhs_call(const int *ex, double T, const double *X, const double *Y, const double *Z, double **u,
@@ -453,11 +490,13 @@ int oracle_bssn_step_single(const int *ex, const double *X, const double *Y, con
  *   sub == 0: input u0, rhs -> K, output -> out
  *   sub >= 1: input in,  rhs -> out (the reference's SynchList_cor), output -> out
  * pbbox is the patch bbox (with buffer) that decides the outer faces.
- * Returns the NaN flag of compute_rhs_bssn.
+ * nf = 25 runs the Z4c right-hand side (Z4c_class::Step, Z4c_class.C:173-1045,
+ * the same sequence with Theta as the 25th field).
+ * Returns the NaN flag of the right-hand side.
  */
-int oracle_bssn_substep(const int *ex, const double *X, const double *Y, const double *Z, const double *pbbox,
-                        double **u0, double **in, double **out, double **K, int sub, double dT, double eps,
-                        double chitiny, int Symmetry, int lev)
+int oracle_evolve_substep(const int *ex, const double *X, const double *Y, const double *Z, const double *pbbox,
+                          double **u0, double **in, double **out, double **K, int sub, double dT, double eps,
+                          double chitiny, int Symmetry, int lev, int nf)
 {
     long n = npts3(ex);
     double *buf = oalloc(n * (24 + 7 + 1));
@@ -469,8 +508,9 @@ int oracle_bssn_substep(const int *ex, const double *X, const double *Y, const d
     double **rtarget = sub == 0 ? K : out;
     oracle_enforce_ga(ex, src[2], src[3], src[4], src[5], src[6], src[7], src[8], src[9], src[10], src[11], src[12],
                       src[13]);
-    int err = rhs_call(ex, 0.0, X, Y, Z, src, rtarget, scr, zero, Symmetry, lev, eps, 1, cons);
-    for (int f = 0; f < 24; ++f) {
+    int err = nf == 25 ? rhs_call_z4c(ex, 0.0, X, Y, Z, src, rtarget, scr, zero, Symmetry, lev, eps, cons)
+                       : rhs_call(ex, 0.0, X, Y, Z, src, rtarget, scr, zero, Symmetry, lev, eps, 1, cons);
+    for (int f = 0; f < nf; ++f) {
         if (lev == 0)
             oracle_sommerfeld_routbam(ex, X, Y, Z, pbbox[0], pbbox[1], pbbox[2], pbbox[3], pbbox[4], pbbox[5],
                                       rtarget[f], src[f], oracle_bssn_propspeed(f), oracle_bssn_soa(f), Symmetry);
@@ -482,4 +522,11 @@ int oracle_bssn_substep(const int *ex, const double *X, const double *Y, const d
     oracle_lowerboundset(ex, out[0], chitiny);
     free(buf);
     return err;
+}
+
+int oracle_bssn_substep(const int *ex, const double *X, const double *Y, const double *Z, const double *pbbox,
+                        double **u0, double **in, double **out, double **K, int sub, double dT, double eps,
+                        double chitiny, int Symmetry, int lev)
+{
+    return oracle_evolve_substep(ex, X, Y, Z, pbbox, u0, in, out, K, sub, dT, eps, chitiny, Symmetry, lev, 24);
 }

@@ -76,4 +76,5 @@ def test_graph_replay_equals_eager():
     e.run_graph(0, dt, nsteps=2, replays=2)
     assert e.sync() == 0
     assert np.array_equal(e.get_state(b), eager)
-    assert e.launches == 4 * 10   # per step: enforce pass, 4 x (stencil pass + pointwise pass), ring rotation
+    # per step: enforce pass, 4 x (stencil pass + pointwise pass + face pass), ring rotation
+    assert e.launches == 4 * 14
