@@ -70,8 +70,16 @@ def workload(name):
 
 
 def make_initial(w, nf=24):
+    """The workload's initial state per block: get_lousto_nbhs_ on the GPU plus
+    the per-cell seeded noise (amss_b200.initial)."""
+    from amss_b200 import initial
+    return initial.initial_state(w["H"], w["masses"], w["pos"], noise=w["noise"], seed=1, nf=nf)
+
+
+def make_initial_reference(w, nf=24):
+    """The same initial state from the oracle's restatement (reference arm)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import amr as OA   # initial data only (Brill-Lindquist, get_lousto_nbhs)
+    import amr as OA
     return OA.initial_state(w["H"], w["masses"], w["pos"], noise=w["noise"], seed=1, nf=nf)
 
 
@@ -309,7 +317,7 @@ def run_reference(args, rank, world):
     w = workload(args.workload)
     H = w["H"]
     nf = 25 if args.formulation == "z4c" else 24
-    init = make_initial(w, nf)
+    init = make_initial_reference(w, nf)
     oh = OA.OracleHierarchy(H, eps=w["eps"], nf=nf)
     for i, st in enumerate(init):
         oh.set_state(i, st)

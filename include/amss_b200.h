@@ -162,6 +162,28 @@ void enforce_ga_(int* ex, double* dxx, double* gxy, double* gxz, double* dyy, do
  * bssn_class.C:3156 and :3525). In place. */
 void lowerboundset_(int* ex, double* chi, double* tinny);
 
+/* Replaces get_lousto_nbhs (initial_puncture.f90:1970-2202; C prototype
+ * initial_puncture.h:165-174, called per block from bssn_class.C:1165):
+ * Lousto's approximate puncture data for N punctures (Mass[N], Porg/Pmom/Spin
+ * [3N]; zero momenta and spins give Brill-Lindquist), stored as offsets
+ * (chi - 1, Lap - 1; metric offsets, trK, Gam, beta, dtSf zero).  The reference
+ * prototype returns void; this one returns 0 or an AMSS_ERR_* code, which a
+ * caller using the void prototype may ignore.  At most 16 punctures. */
+int get_lousto_nbhs_(int* ex, double* X, double* Y, double* Z, double* chi, double* trK,
+                     double* gxx, double* gxy, double* gxz, double* gyy, double* gyz, double* gzz,
+                     double* Axx, double* Axy, double* Axz, double* Ayy, double* Ayz, double* Azz,
+                     double* Gmx, double* Gmy, double* Gmz, double* Lap, double* Sfx, double* Sfy, double* Sfz,
+                     double* dtSfx, double* dtSfy, double* dtSfz, double* Mass, double* Porg, double* Pmom,
+                     double* Spin, int* N);
+
+/* No counterpart in the reference.  The vector-Jacobian product of
+ * get_lousto_nbhs_ with zero momenta and spins (Brill-Lindquist) with respect
+ * to the masses and positions: given the adjoints chi_b, lap_b of the chi and
+ * Lap outputs (host, Fortran order), dMass[N] and dPorg[3N].  The other outputs
+ * do not depend on them in this case. */
+int amss_lousto_vjp(const int* ex, const double* X, const double* Y, const double* Z, int N, const double* Mass,
+                    const double* Porg, const double* chi_b, const double* lap_b, double* dMass, double* dPorg);
+
 /* ---------------------------------------------------------------------------
  * Batched engine: device-resident blocks, one launch per level substep.
  * ------------------------------------------------------------------------- */
@@ -248,6 +270,31 @@ void* amss_engine_stream(amss_engine* e);
 
 /* Number of kernel launches the engine issued so far. */
 long long amss_engine_launch_count(amss_engine* e);
+
+/* ---- Adjoint of a single-patch BSSN evolution (no reference counterpart:
+ * the reference has no derivative code; the forward it differentiates is the
+ * level-0 RK4 step of bssn_class::Step, bssn_class.C:2981-3700, with
+ * enforce_ga, lowerboundset and the Sommerfeld outer boundary).
+ *
+ * One block of ex points per direction on its cell-centred bbox, FP64,
+ * GAUGE 0, no symmetry.  The loss is L = sum over the cells at least 3 cells
+ * from every face of H^2 dx dy dz, H the Hamiltonian constraint of the final
+ * state.  The gradient is dL/d(initial state) (24 fields, field-major, the
+ * same host layout as amss_engine_set_state), computed by reverse-mode over
+ * RK4 with a checkpoint every `ck` steps (each segment recomputed once). */
+typedef struct amss_adjoint amss_adjoint;
+
+/* chitiny: the lowerboundset floor on chi (bssn_class.C:179, :3156).  NULL on failure. */
+amss_adjoint* amss_adjoint_create(const int ex[3], const double bbox[6], double eps, double chitiny);
+void amss_adjoint_destroy(amss_adjoint* a);
+int amss_adjoint_set_state(amss_adjoint* a, const double* host_state);
+int amss_adjoint_get_state(amss_adjoint* a, double* host_state);
+/* nsteps RK4 steps of dt from the state set; *loss = L of the final state. */
+int amss_adjoint_forward(amss_adjoint* a, double dt, int nsteps, int ck, double* loss);
+/* dL/d(state before the last amss_adjoint_forward) into host_grad (24 fields). */
+int amss_adjoint_backward(amss_adjoint* a, double* host_grad);
+void* amss_adjoint_stream(amss_adjoint* a);
+long long amss_adjoint_launch_count(amss_adjoint* a);
 
 #ifdef __cplusplus
 }

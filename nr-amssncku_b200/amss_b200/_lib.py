@@ -58,6 +58,21 @@ def lib():
     L.amss_engine_level_points.restype = ctypes.c_longlong
     L.amss_engine_launch_count.argtypes = [ctypes.c_void_p]
     L.amss_engine_launch_count.restype = ctypes.c_longlong
+    L.get_lousto_nbhs_.restype = ctypes.c_int
+    L.amss_lousto_vjp.restype = ctypes.c_int
+    L.amss_lousto_vjp.argtypes = [_IP, _DP, _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]
+    L.amss_adjoint_create.restype = ctypes.c_void_p
+    L.amss_adjoint_create.argtypes = [_IP, _DP, ctypes.c_double, ctypes.c_double]
+    L.amss_adjoint_destroy.restype = None
+    L.amss_adjoint_destroy.argtypes = [ctypes.c_void_p]
+    L.amss_adjoint_set_state.argtypes = [ctypes.c_void_p, _DP]
+    L.amss_adjoint_get_state.argtypes = [ctypes.c_void_p, _DP]
+    L.amss_adjoint_forward.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, _DP]
+    L.amss_adjoint_backward.argtypes = [ctypes.c_void_p, _DP]
+    L.amss_adjoint_stream.restype = ctypes.c_void_p
+    L.amss_adjoint_stream.argtypes = [ctypes.c_void_p]
+    L.amss_adjoint_launch_count.restype = ctypes.c_longlong
+    L.amss_adjoint_launch_count.argtypes = [ctypes.c_void_p]
     _lib = L
     return L
 

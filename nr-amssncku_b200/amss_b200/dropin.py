@@ -132,3 +132,36 @@ def enforce_ga(state):
 def lowerboundset(chi, tiny):
     """lowerboundset (fmisc.f90:1644-1657) in place."""
     lib().lowerboundset_(_ex(chi.shape), _p(chi), ctypes.byref(ctypes.c_double(tiny)))
+
+
+def get_lousto_nbhs(X, Y, Z, masses, positions, momenta=None, spins=None):
+    """get_lousto_nbhs (initial_puncture.f90:1970-2202) on the GPU: the 24-field
+    state (offsets) of N punctures; zero momenta and spins give Brill-Lindquist."""
+    X, Y, Z = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, Y, Z))
+    m = np.ascontiguousarray(masses, dtype=np.float64).reshape(-1)
+    n = len(m)
+    porg = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+    pmom = np.zeros(3 * n) if momenta is None else np.ascontiguousarray(momenta, dtype=np.float64).reshape(-1)
+    spin = np.zeros(3 * n) if spins is None else np.ascontiguousarray(spins, dtype=np.float64).reshape(-1)
+    if porg.size != 3 * n or pmom.size != 3 * n or spin.size != 3 * n:
+        raise AmssError("positions, momenta and spins need 3 values per puncture")
+    st = np.empty((24, len(Z), len(Y), len(X)))
+    check(lib().get_lousto_nbhs_((ctypes.c_int * 3)(len(X), len(Y), len(Z)), _p(X), _p(Y), _p(Z),
+                                 *[_p(st[f]) for f in range(24)], _p(m), _p(porg), _p(pmom), _p(spin),
+                                 ctypes.byref(ctypes.c_int(n))), "get_lousto_nbhs_")
+    return st
+
+
+def lousto_vjp(X, Y, Z, masses, positions, state_b):
+    """Adjoints of the Brill-Lindquist masses and positions for the state
+    adjoint state_b (24, ex[2], ex[1], ex[0]): (dmass[N], dpos[N, 3])."""
+    X, Y, Z = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, Y, Z))
+    m = np.ascontiguousarray(masses, dtype=np.float64).reshape(-1)
+    porg = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+    chi_b = np.ascontiguousarray(state_b[0], dtype=np.float64)
+    lap_b = np.ascontiguousarray(state_b[17], dtype=np.float64)
+    dm = np.zeros(len(m))
+    dp = np.zeros(3 * len(m))
+    check(lib().amss_lousto_vjp((ctypes.c_int * 3)(len(X), len(Y), len(Z)), _p(X), _p(Y), _p(Z), len(m), _p(m),
+                                _p(porg), _p(chi_b), _p(lap_b), _p(dm), _p(dp)), "amss_lousto_vjp")
+    return dm, dp.reshape(-1, 3)

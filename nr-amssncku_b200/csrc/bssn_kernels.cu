@@ -13,6 +13,7 @@
 
 #include "bssn_step.cuh"
 #include "amss_b200.h"
+#include "dropin_ctx.cuh"
 #include "dev_util.cuh"
 #include "substep_impl.cuh"
 
@@ -172,38 +173,8 @@ void block_faces(const int ex[3], const double* X, const double* Y, const double
   *lowsym_mask = ls;
 }
 
-// Per-thread device scratch of the drop-in entries (grow-only, reused).
-struct DropinCtx {
-  cudaStream_t stream = nullptr;
-  double* dbuf = nullptr;
-  size_t cap = 0;      // doubles
-  unsigned* dstatus = nullptr;
-  bool ok = false;
-  ~DropinCtx() {
-    if (dbuf) cudaFree(dbuf);
-    if (dstatus) cudaFree(dstatus);
-    if (stream) cudaStreamDestroy(stream);
-  }
-  int init() {
-    if (ok) return 0;
-    if (check_device("drop-in") != 0) return -1;
-    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
-    if (cudaMalloc(&dstatus, sizeof(unsigned)) != cudaSuccess) return -1;
-    ok = true;
-    return 0;
-  }
-  double* reserve(size_t n) {
-    if (n > cap) {
-      if (dbuf) cudaFree(dbuf);
-      dbuf = nullptr;
-      cap = 0;
-      if (cudaMalloc(&dbuf, n * sizeof(double)) != cudaSuccess) return nullptr;
-      cap = n;
-    }
-    return dbuf;
-  }
-};
 static thread_local DropinCtx g_ctx;
+DropinCtx& dropin_ctx() { return g_ctx; }
 
 static int grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;

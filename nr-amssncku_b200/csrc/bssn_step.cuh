@@ -21,23 +21,25 @@
 
 namespace amss {
 
-// enforce_algebra.f90:72-133 on one point (double).
-__device__ __forceinline__ void enforce_ga_point(double* g, double* a) {
+// enforce_algebra.f90:72-133 on one point (double; a recording scalar type for
+// the adjoint generator).
+template <typename T = double>
+__device__ __forceinline__ void enforce_ga_point(T* g, T* a) {
   // g = {dxx, gxy, gxz, dyy, gyz, dzz}, a = {Axx, Axy, Axz, Ayy, Ayz, Azz}
   const double F1o3 = 1.0 / 3.0, ONE = 1.0, TWO = 2.0;
-  double gxx = g[0] + ONE, gyy = g[3] + ONE, gzz = g[5] + ONE;
-  double gxy = g[1], gxz = g[2], gyz = g[4];
-  double d = gxx * gyy * gzz + gxy * gyz * gxz + gxz * gxy * gyz - gxz * gyy * gxz - gxy * gxy * gzz - gxx * gyz * gyz;
+  T gxx = g[0] + ONE, gyy = g[3] + ONE, gzz = g[5] + ONE;
+  T gxy = g[1], gxz = g[2], gyz = g[4];
+  T d = gxx * gyy * gzz + gxy * gyz * gxz + gxz * gxy * gyz - gxz * gyy * gxz - gxy * gxy * gzz - gxx * gyz * gyz;
   d = ONE / pow(d, F1o3);
   gxx = gxx * d; gxy = gxy * d; gxz = gxz * d; gyy = gyy * d; gyz = gyz * d; gzz = gzz * d;
   g[0] = gxx - ONE; g[1] = gxy; g[2] = gxz; g[3] = gyy - ONE; g[4] = gyz; g[5] = gzz - ONE;
-  const double uxx = (gyy * gzz - gyz * gyz);
-  const double uxy = -(gxy * gzz - gyz * gxz);
-  const double uxz = (gxy * gyz - gyy * gxz);
-  const double uyy = (gxx * gzz - gxz * gxz);
-  const double uyz = -(gxx * gyz - gxy * gxz);
-  const double uzz = (gxx * gyy - gxy * gxy);
-  const double trA = uxx * a[0] + uyy * a[3] + uzz * a[5] + TWO * (uxy * a[1] + uxz * a[2] + uyz * a[4]);
+  const T uxx = (gyy * gzz - gyz * gyz);
+  const T uxy = -(gxy * gzz - gyz * gxz);
+  const T uxz = (gxy * gyz - gyy * gxz);
+  const T uyy = (gxx * gzz - gxz * gxz);
+  const T uyz = -(gxx * gyz - gxy * gxz);
+  const T uzz = (gxx * gyy - gxy * gxy);
+  const T trA = uxx * a[0] + uyy * a[3] + uzz * a[5] + TWO * (uxy * a[1] + uxz * a[2] + uyz * a[4]);
   a[0] = a[0] - F1o3 * gxx * trA;
   a[1] = a[1] - F1o3 * gxy * trA;
   a[2] = a[2] - F1o3 * gxz * trA;

@@ -78,6 +78,8 @@ class Tape:
                 v[i] = v[self.a[i]] / v[self.b[i]]
             elif op == "n":
                 v[i] = -v[self.a[i]]
+            elif op == "p":
+                v[i] = v[self.a[i]] ** v[self.b[i]]
             else:
                 raise ValueError(op)
         return {f: v[i] for f, i in self.outputs.items()}
@@ -107,6 +109,8 @@ def vjp(tape, c, d, rb):
             v[i] = v[tape.a[i]] / v[tape.b[i]]
         elif op == "n":
             v[i] = -v[tape.a[i]]
+        elif op == "p":
+            v[i] = v[tape.a[i]] ** v[tape.b[i]]
     adj = [None] * n
 
     def add(j, x):
@@ -134,6 +138,8 @@ def vjp(tape, c, d, rb):
         elif op == "/":
             add(a, g / v[b])
             add(b, -(g * v[i] / v[b]))
+        elif op == "p":
+            add(a, g * v[b] * v[i] / v[a])
     cb = {f: adj[i] for f, i in tape.inputs_c.items() if adj[i] is not None}
     db = {s: adj[i] for s, i in tape.inputs_d.items() if adj[i] is not None}
     return cb, db
@@ -163,6 +169,8 @@ def emit_vjp(tape, name):
             w(f"  const T v{i} = in.d({tape.a[i]});")
         elif op == "n":
             w(f"  const T v{i} = -{val(tape.a[i])};")
+        elif op == "p":
+            w(f"  const T v{i} = pow({val(tape.a[i])}, {val(tape.b[i])});")
         else:
             w(f"  const T v{i} = {val(tape.a[i])} {op} {val(tape.b[i])};")
     # reverse sweep
@@ -205,12 +213,40 @@ def emit_vjp(tape, name):
         elif op == "/":
             add(a, f"a{i} / {val(b)}")
             add(b, f"a{i} * v{i} / {val(b)}", neg=True)
+        elif op == "p":
+            add(a, f"a{i} * {val(b)} * v{i} / {val(a)}")
     for f, i in sorted(tape.inputs_c.items()):
         if i in defined:
             w(f"  out.cb({f}, a{i});")
     for s, i in sorted(tape.inputs_d.items()):
         if i in defined:
             w(f"  out.db({s}, a{i});")
+    w("}")
+    return "\n".join(L) + "\n"
+
+
+def emit_fwd(tape, name, field):
+    """CUDA source of `name`: the tape's output `field` as a function of in.c /
+    in.d (template <typename T, typename In> __device__ T name(const In& in))."""
+    L = []
+    w = L.append
+    val = lambda i: (repr_k(tape.val[i]) if tape.op[i] == "k" else f"v{i}")
+    w(f"template <typename T, typename In>")
+    w(f"__device__ __forceinline__ T {name}(const In& in) {{")
+    for i, op in enumerate(tape.op):
+        if not tape.live[i] or op == "k":
+            continue
+        if op == "c":
+            w(f"  const T v{i} = in.c({tape.a[i]});")
+        elif op == "d":
+            w(f"  const T v{i} = in.d({tape.a[i]});")
+        elif op == "n":
+            w(f"  const T v{i} = -{val(tape.a[i])};")
+        elif op == "p":
+            w(f"  const T v{i} = pow({val(tape.a[i])}, {val(tape.b[i])});")
+        else:
+            w(f"  const T v{i} = {val(tape.a[i])} {op} {val(tape.b[i])};")
+    w(f"  return {val(tape.outputs[field])};")
     w("}")
     return "\n".join(L) + "\n"
 

@@ -12,7 +12,7 @@
 //   <id> in c <field>        centre value of a field
 //   <id> in d <slot>         D slot
 //   <id> k <value>           constant (hex float)
-//   <id> <op> <a> <b>        add sub mul div (b unused for neg)
+//   <id> <op> <a> <b>        + - * / ; n negate (b unused); p power (b: constant exponent)
 //   out <field> <id>
 // so the generated adjoint differentiates exactly what the forward computes.
 #include <cmath>
@@ -71,8 +71,10 @@ inline bool operator!=(Rec, Rec) { return false; }
 inline bool operator>(Rec, Rec) { return false; }
 inline bool operator<(Rec, Rec) { return false; }
 inline bool isinf(Rec) { return false; }
+// x^c for a constant exponent c (enforce_ga's det^(1/3))
+inline Rec pow(Rec x, double c) { return Rec::of(trace::push('p', x.id, trace::konst(c))); }
 
-#include "../csrc/bssn_rhs.cuh"
+#include "../csrc/bssn_step.cuh"
 
 namespace amss {
 template <>
@@ -123,7 +125,8 @@ struct RecHamEpi {
 };
 
 int main(int argc, char** argv) {
-  // argument: "bssn" (default), "z4c", or "ham" (the Hamiltonian constraint)
+  // argument: "bssn" (default), "z4c", "ham" (the Hamiltonian constraint) or
+  // "enforce" (enforce_ga_point)
   const char mode = argc > 1 ? argv[1][0] : 'b';
   RecPt q;
   Coefs<Rec> C{};
@@ -131,7 +134,19 @@ int main(int argc, char** argv) {
   G.ord = 2;
   RhsAux aux{};
   std::map<int, int> out;
-  if (mode == 'h') {
+  if (mode == 'e') {
+    // enforce_ga_point: inputs c0..c5 = the metric offsets, c6..c11 = A~_ij
+    Rec gv[6], av[6];
+    for (int m = 0; m < 6; ++m) {
+      gv[m] = Rec::of(trace::push('c', m, -1));
+      av[m] = Rec::of(trace::push('c', 6 + m, -1));
+    }
+    enforce_ga_point(gv, av);
+    for (int m = 0; m < 6; ++m) {
+      out[m] = gv[m].id;
+      out[6 + m] = av[m].id;
+    }
+  } else if (mode == 'h') {
     RecHamEpi epi{&out};
     bssn_rhs_point<Rec, Rec, false, false, false>(q, C, G, aux, epi);
   } else {

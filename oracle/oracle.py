@@ -185,18 +185,25 @@ def sommerfeld_rout_freeze(X, Y, Z, bbox, f0, f, symmetry=0):
                                         _p(f0), _p(f), ctypes.c_int(symmetry), ctypes.c_int(1))
 
 
-def brill_lindquist(X, Y, Z, masses, positions):
-    """get_lousto_nbhs with zero momenta and spins: the Brill-Lindquist data."""
+def get_lousto_nbhs(X, Y, Z, masses, positions, momenta=None, spins=None):
+    """initial_puncture.f90:1970-2202: the 24-field state of N punctures."""
     ex = (len(X), len(Y), len(Z))
     st = np.zeros((24, ex[2], ex[1], ex[0]))
-    m = np.asarray(masses, dtype=np.float64)
-    porg = np.asarray(positions, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(masses, dtype=np.float64).reshape(-1)
+    porg = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
     zeros = np.zeros(3 * len(m))
+    pmom = zeros if momenta is None else np.ascontiguousarray(momenta, dtype=np.float64).reshape(-1)
+    spin = zeros if spins is None else np.ascontiguousarray(spins, dtype=np.float64).reshape(-1)
     ptrs = (_DP * 24)(*[_p(st[f]) for f in range(24)])
     lib().oracle_get_lousto_nbhs((ctypes.c_int * 3)(*ex), _p(np.ascontiguousarray(X)), _p(np.ascontiguousarray(Y)),
-                                 _p(np.ascontiguousarray(Z)), ptrs, _p(m), _p(porg), _p(zeros), _p(zeros),
+                                 _p(np.ascontiguousarray(Z)), ptrs, _p(m), _p(porg), _p(pmom), _p(spin),
                                  ctypes.c_int(len(m)))
     return st
+
+
+def brill_lindquist(X, Y, Z, masses, positions):
+    """get_lousto_nbhs with zero momenta and spins: the Brill-Lindquist data."""
+    return get_lousto_nbhs(X, Y, Z, masses, positions)
 
 
 def l2normhelper(X, Y, Z, bbox, f, gw):

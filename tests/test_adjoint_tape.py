@@ -1,10 +1,11 @@
 """The straight-line programs the adjoint is generated from (no GPU).
 
-gen/tape_{bssn,z4c}.txt are recordings of the kernel's own point function
-(bssn_rhs_point, split form) by gen/trace_rhs.cpp.  Fed with the stencil terms
-the oracle's fderivs / fdderivs / lopsided / kodis produce, the tape must give
-the oracle's right-hand side; its reverse sweep must agree with central
-finite differences of the tape.
+gen/tape_*.txt are recordings of the kernels' own point functions by
+gen/trace_rhs.cpp: the split-form right-hand side (bssn_rhs_point, BSSN and
+Z4c), the Hamiltonian constraint and enforce_ga_point.  Fed with the stencil
+terms the oracle's fderivs / fdderivs / lopsided / kodis produce, a tape must
+give the oracle's values; its reverse sweep must agree with central finite
+differences of the tape.
 """
 import os
 import sys
@@ -80,15 +81,42 @@ def test_tape_forward_matches_oracle_rhs(z4c):
         assert err <= 1e-12, (f, err)
 
 
-@pytest.mark.parametrize("z4c", [False, True])
-def test_tape_reverse_sweep_matches_finite_differences(z4c):
+def _tape(name):
+    return TP.Tape(os.path.join(HERE, "..", "nr-amssncku_b200", "gen", f"tape_{name}.txt"))
+
+
+def test_ham_tape_matches_oracle_constraint():
+    X = O.cell_coords(-2.0, 2.5, 18)
+    Y = O.cell_coords(-1.5, 2.0, 16)
+    Z = O.cell_coords(-3.0, 1.0, 14)
+    st = generic_state(X, Y, Z, seed=9)
+    ref = O.compute_rhs_bssn(X, Y, Z, st, eps=0.1, co=0)[4][0]
+    out = _tape("ham").evaluate({f: st[f] for f in range(24)}, stencil_terms(X, Y, Z, st, 0.1, False))
+    assert np.abs(out[99] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_enforce_tape_matches_oracle():
+    rng = np.random.default_rng(5)
+    st = np.zeros((24, 4, 5, 6))
+    for f in range(2, 14):
+        st[f] = rng.uniform(-0.1, 0.1, st.shape[1:])
+    ref = st.copy()
+    O.enforce_ga(ref)
+    out = _tape("enforce").evaluate({m: st[2 + m] for m in range(12)}, {})
+    for m in range(12):
+        assert np.abs(out[m] - ref[2 + m]).max() <= 1e-14, m
+
+
+@pytest.mark.parametrize("name", ["bssn", "z4c", "ham", "enforce"])
+def test_tape_reverse_sweep_matches_finite_differences(name):
     """<rb, J dx> from central differences of the tape equals <J^T rb, dx>."""
-    tp = TP.Tape(os.path.join(HERE, "..", "nr-amssncku_b200", "gen", "tape_z4c.txt" if z4c else "tape_bssn.txt"))
+    tp = _tape(name)
     rng = np.random.default_rng(3)
     npt = 64
     c = {f: rng.uniform(-0.1, 0.1, npt) for f in tp.inputs_c}
-    c[0] = rng.uniform(-0.5, -0.3, npt)       # chi - 1
-    c[17] = rng.uniform(-0.4, -0.2, npt)      # alpha - 1
+    if name != "enforce":
+        c[0] = rng.uniform(-0.5, -0.3, npt)       # chi - 1
+        c[17] = rng.uniform(-0.4, -0.2, npt)      # alpha - 1
     d = {s: rng.uniform(-0.2, 0.2, npt) for s in tp.inputs_d}
     rb = {f: rng.standard_normal(npt) for f in tp.outputs}
     dc = {f: rng.standard_normal(npt) for f in c}
