@@ -306,6 +306,93 @@ def cpu_baseline(args, w, init, budget_s=12.0):
                       f"zones), FP64, OpenMP over {cores} threads"}
 
 
+def run_adjoint(args):
+    """adjoint96: the gradient of L = sum_interior H^2 dV after 200 FP64 RK4
+    steps (checkpoint every 20) on one 96^3-interior block on [-12, 12]^3,
+    Brill-Lindquist m = 1 at (0.1, 0.05, 0.02) plus a Gaussian on gamma~_xx
+    (amplitude 1e-4, width 2, centre uniform in the ball r < 4, seed 1).
+    Reports the adjoint step (reverse sweep incl. the segment recompute, per
+    step) over the forward step (with checkpointing), and over the engine's
+    FP64 step of the same block."""
+    import torch
+    import amss_b200
+    from amss_b200 import initial
+    from amss_b200.adjoint import Adjoint
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, nsteps, ck = args.adj_n, args.adj_steps, args.adj_ck
+    X, st, bbox, h = initial.single_block_state(n, -n / 8.0, n / 8.0, 3, [1.0], [[0.1, 0.05, 0.02]])
+    rng = np.random.default_rng(1)
+    while True:
+        c = rng.uniform(-4.0, 4.0, 3)
+        if np.linalg.norm(c) < 4.0:
+            break
+    st[2] += initial.gaussian(X, X, X, 1e-4, 2.0, c)
+    dt = 0.25 * h
+    ex = (len(X),) * 3
+    adj = Adjoint(ex, bbox)
+    stream = torch.cuda.ExternalStream(adj.stream)
+    for _ in range(args.warmup):
+        adj.set_state(st)
+        adj.forward(dt, 2, 1)
+        adj.backward()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), out
+
+    fwd, bwd = [], []
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for _ in range(args.steps):
+            adj.set_state(st)
+            l0 = adj.launches
+            t, loss = timed(lambda: adj.forward(dt, nsteps, ck))
+            fwd.append(t)
+            lf = adj.launches - l0
+            t, grad = timed(adj.backward)
+            bwd.append(t)
+            lb = adj.launches - l0 - lf
+    adj.close()
+    # the engine's FP64 step of the same block (split kernels, CUDA graph)
+    eng = amss_b200.Engine(precision="fp64")
+    b = eng.add_block(0, ex, bbox, bbox)
+    eng.commit()
+    eng.set_state(b, st)
+    es = torch.cuda.ExternalStream(eng.stream)
+    eng.run_graph(0, dt, 20, 1)
+    eng.sync()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    eng.set_state(b, st)
+    torch.cuda.synchronize()
+    a.record(es)
+    eng.run_graph(0, dt, nsteps, 1)
+    e.record(es)
+    torch.cuda.synchronize()
+    eng_ms = a.elapsed_time(e) / nsteps
+    eng.close()
+    f_ms = max(fwd) / nsteps
+    b_ms = max(bwd) / nsteps
+    zones = n ** 3
+    return {
+        "metric": f"adjoint step time / forward step time (FP64, {n}^3, {nsteps} RK4 steps, checkpoint every {ck})",
+        "value": round(b_ms / f_ms, 3), "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic (Brill-Lindquist + "
+        "Gaussian on gamma~_xx, generated in-process)",
+        "forward_ms_per_step": round(f_ms, 4), "adjoint_ms_per_step": round(b_ms, 4),
+        "engine_forward_ms_per_step": round(eng_ms, 4), "adjoint_vs_engine_step": round(b_ms / eng_ms, 3),
+        "forward_zone_updates_per_s": zones / (f_ms * 1e-3), "loss": loss,
+        "grad_norm": float(np.sqrt(np.sum(grad ** 2))),
+        "gpu_launches": {"forward": int(lf), "backward": int(lb)}, "clocks": clk.summary(),
+        "config": {"workload": "adjoint96: 96^3 interior + 3 ghosts on [-12,12]^3, BL m=1 at (0.1,0.05,0.02) + "
+                               "Gaussian on gamma~_xx (1e-4, width 2), dt=0.25dx, 200 FP64 RK4 steps, checkpoint "
+                               "every 20, loss sum_interior H^2 dV"},
+    }
+
+
 def run_reference(args, rank, world):
     """The reference arm: the oracle (the C restatement of the reference's
     Fortran) on all host cores, one finest-level RK4 step of the workload per
@@ -355,15 +442,25 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--workload", default="amr",
-                    help="amr | amr8 | singleN (one block of N^3 interior cells, e.g. single64, single320)")
+                    help="amr | amr8 | singleN (one block of N^3 interior cells, e.g. single64, single320) | "
+                         "adjoint96 (adjoint / forward step time)")
     ap.add_argument("--formulation", choices=["bssn", "z4c"], default="bssn")
     ap.add_argument("--kernel", choices=["split", "fused"], default="split")
     ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adj-n", type=int, default=96, help="adjoint96: interior cells per side (smaller for ncu)")
+    ap.add_argument("--adj-steps", type=int, default=200, help="adjoint96: RK4 steps")
+    ap.add_argument("--adj-ck", type=int, default=20, help="adjoint96: checkpoint interval")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "adjoint96":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}))
+        elif rank == 0:
+            print(json.dumps(run_adjoint(args)))
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
         if line is not None:

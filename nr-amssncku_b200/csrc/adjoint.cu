@@ -16,7 +16,7 @@
 //   s = 3, 2, 1:  Xb_s = F'(X_s)^T R_sb;  Zb = mask(Z_{s-1}) E'(Z_{s-1})^T Xb_s;
 //                 U0b += Zb;  R_{s-1}b += c_{s-1} Zb        (c = dt/2, dt/2, dt)
 //   U0b += F'(X_0)^T R0b;  Ub(previous step) = E'(U0 raw)^T U0b.
-// F'^T is k_rhs_vjp (pointwise, generated) + k_stencil_vjp (stencil
+// F'^T is k_rhs_vjp (pointwise, generated) + k_stencil_gather (stencil
 // transpose) + k_face_vjp (Sommerfeld transpose); E'^T and the floor mask are
 // k_enforce_vjp.
 #include <cmath>
@@ -59,24 +59,6 @@ __global__ void k_enforce_copy(const double* __restrict__ in, double* __restrict
   }
 }
 
-// y = a * mask(Z) * x (chi masked where Z_chi sits at the floor); n fields
-__global__ void k_scale_mask(const double* __restrict__ x, const double* __restrict__ Z, double* __restrict__ y,
-                             double a, long long n, long long fs, double chitiny, int accumulate) {
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
-    for (int f = 0; f < NFIELDS_BSSN; ++f) {
-      double v = a * x[f * fs + p];
-      if (f == F_CHI && Z[f * fs + p] == chitiny) v = 0.0;
-      if (accumulate) y[f * fs + p] += v;
-      else y[f * fs + p] = v;
-    }
-}
-
-// y += a * x over m contiguous doubles
-__global__ void k_axpy(const double* __restrict__ x, double* __restrict__ y, double a, long long m) {
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (long long)gridDim.x * blockDim.x)
-    y[q] += a * x[q];
-}
-
 }  // namespace amss
 
 using namespace amss;
@@ -115,7 +97,6 @@ struct amss_adjoint {
   double* U0b = nullptr;
   double* Rb[4] = {nullptr, nullptr, nullptr, nullptr};
   double* Xb = nullptr;
-  double* Zb = nullptr;
   double dt = 0;
   int nsteps = 0, ck = 1;
   bool forward_done = false;
@@ -189,15 +170,16 @@ int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, doub
   a->host_adj.Rb = Rbv;
   a->host_adj.Xb = Xbv;
   AMSS_CK(cudaMemcpyAsync(a->dadj, &a->host_adj, sizeof(AdjBlock), cudaMemcpyHostToDevice, s));
-  AMSS_CK(cudaMemsetAsync(Xbv, 0, state_bytes(a), s));
-  AMSS_CK(cudaMemsetAsync(a->Db, 0, (size_t)D_SLOTS * a->fs * sizeof(double), s));
   k_rhs_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, a->Db);
   AMSS_CK(cudaGetLastError());
-  k_stencil_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, a->Db, D_SLOTS);
+  k_stencil_gather<<<dim3(grid_of(a->npts), NFIELDS_BSSN), 128, 0, s>>>(a->dadj, a->Db);
+  AMSS_CK(cudaGetLastError());
+  k_beta_adjoint<<<grid_of(a->npts), 128, 0, s>>>(a->dadj, a->Db);
   AMSS_CK(cudaGetLastError());
   if (a->nfaces) {
     k_face_vjp<<<grid_of(a->nfaces), 128, 0, s>>>(a->dadj, a->dfaces, a->nfaces);
     AMSS_CK(cudaGetLastError());
+    a->launches++;
   }
   a->launches += 4;
   return 0;
@@ -208,6 +190,10 @@ int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, doub
 extern "C" amss_adjoint* amss_adjoint_create(const int ex[3], const double bbox[6], double eps, double chitiny) {
   if (!ex || ex[0] < kDerivMinEx || ex[1] < 7 || ex[2] < 7) {
     amss_fail(AMSS_ERR_ARG, "amss_adjoint_create: needs ex[0] >= 8 and ex[1], ex[2] >= 7");
+    return nullptr;
+  }
+  if ((long long)ex[0] * ex[1] * ex[2] * D_SLOTS >= (1LL << 31) - (1LL << 26)) {
+    amss_fail(AMSS_ERR_ARG, "amss_adjoint_create: block too large (the stencil adjoints use 32-bit offsets)");
     return nullptr;
   }
   if (check_device("amss_adjoint_create") != 0) return nullptr;
@@ -240,7 +226,7 @@ extern "C" amss_adjoint* amss_adjoint_create(const int ex[3], const double bbox[
       cudaMalloc(&a->H, a->fs * sizeof(double)) != cudaSuccess || cudaMalloc(&a->dloss, sizeof(double)) != cudaSuccess)
     return fail("amss_adjoint_create: device allocation failed");
   double** bufs[] = {&a->U, &a->U0, &a->X[0], &a->X[1], &a->X[2], &a->K, &a->Ub, &a->U0b,
-                     &a->Rb[0], &a->Rb[1], &a->Rb[2], &a->Rb[3], &a->Xb, &a->Zb};
+                     &a->Rb[0], &a->Rb[1], &a->Rb[2], &a->Rb[3], &a->Xb};
   for (double** b : bufs)
     if (cudaMalloc(b, sb) != cudaSuccess) return fail("amss_adjoint_create: device allocation failed");
   if (cudaMalloc(&a->Zs, 3 * sb) != cudaSuccess) return fail("amss_adjoint_create: device allocation failed");
@@ -310,7 +296,7 @@ extern "C" void amss_adjoint_destroy(amss_adjoint* a) {
   if (a->stream) cudaStreamSynchronize(a->stream);
   void* ptrs[] = {a->dstatus, a->dlvl, a->dcoord, a->dtab, a->dadj, a->ditems, a->dtiles, a->dfaces, a->D, a->Db,
                   a->U, a->U0, a->X[0], a->X[1], a->X[2], a->K, a->Zs, a->H, a->dloss, a->seg, a->Ub, a->U0b,
-                  a->Rb[0], a->Rb[1], a->Rb[2], a->Rb[3], a->Xb, a->Zb};
+                  a->Rb[0], a->Rb[1], a->Rb[2], a->Rb[3], a->Xb};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* c : a->ckpt) cudaFree(c);
@@ -356,7 +342,7 @@ static int loss_and_grad(amss_adjoint* a, double* loss, bool want_grad) {
     AMSS_CK(cudaMemsetAsync(a->Db, 0, (size_t)D_SLOTS * a->fs * sizeof(double), s));
     k_ham_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, gw, dV, a->H, a->Db);
     AMSS_CK(cudaGetLastError());
-    k_stencil_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, a->Db, D_SLOTS);
+    k_stencil_gather<<<dim3(grid_of(a->npts), NFIELDS_BSSN), 128, 0, s>>>(a->dadj, a->Db);   // H reads no adv slot
     AMSS_CK(cudaGetLastError());
     a->launches += 2;
   }
@@ -428,27 +414,23 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
       AMSS_CK(cudaGetLastError());
       if (int rc = set_tables(a, Unew, Z[0], Z[1], Z[2])) return rc;
       // U_new = floor(U0 + dt/6 (R0 + 2 R1 + 2 R2 + R3))
-      k_scale_mask<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->U0b, 1.0, n, fs, a->chitiny, 0);
-      k_scale_mask<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->Rb[3], dt / 6.0, n, fs, a->chitiny, 0);
-      k_scale_mask<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->Rb[0], dt / 6.0, n, fs, a->chitiny, 0);
-      k_scale_mask<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->Rb[1], dt / 3.0, n, fs, a->chitiny, 0);
-      k_scale_mask<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->Rb[2], dt / 3.0, n, fs, a->chitiny, 0);
+      k_step_seed<<<grid_of(n), 128, 0, s>>>(a->Ub, Unew, a->U0b, a->Rb[0], a->Rb[1], a->Rb[2], a->Rb[3], dt, n, fs,
+                                             a->chitiny);
       AMSS_CK(cudaGetLastError());
       // substeps 3, 2, 1: X_s = E(Z_{s-1}), Z_{s-1} = floor(U0 + c R_{s-1})
       const double c[3] = {0.5 * dt, 0.5 * dt, dt};
       for (int sub = 3; sub >= 1; --sub) {
         if (int rc = rhs_vjp(a, sub, a->X[sub - 1], a->Rb[sub], a->Xb)) return rc;
-        k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(Z[sub - 1], a->Xb, a->Zb, n, fs, a->chitiny, 1);
-        k_axpy<<<grid_of(m), 128, 0, s>>>(a->Zb, a->U0b, 1.0, m);
-        k_axpy<<<grid_of(m), 128, 0, s>>>(a->Zb, a->Rb[sub - 1], c[sub - 1], m);
+        k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(Z[sub - 1], a->Xb, nullptr, nullptr, a->U0b, a->Rb[sub - 1],
+                                                 c[sub - 1], n, fs, a->chitiny);
         AMSS_CK(cudaGetLastError());
       }
       if (int rc = rhs_vjp(a, 0, a->U0, a->Rb[0], a->Xb)) return rc;
-      k_axpy<<<grid_of(m), 128, 0, s>>>(a->Xb, a->U0b, 1.0, m);
-      // the enforce pass at the start of the step
-      k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(U0raw, a->U0b, a->Ub, n, fs, a->chitiny, 1);
+      // the enforce pass at the start of the step: Ub = E'(U0raw)^T (U0b + Xb)
+      k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(U0raw, a->U0b, a->Xb, a->Ub, nullptr, nullptr, 0.0, n, fs,
+                                               a->chitiny);
       AMSS_CK(cudaGetLastError());
-      a->launches += 20;
+      a->launches += 9;
     }
   }
   AMSS_CK(cudaMemcpy2DAsync(grad, n * sizeof(double), a->Ub, fs * sizeof(double), n * sizeof(double), NFIELDS_BSSN,

@@ -80,127 +80,13 @@ struct VjpIn {
   __device__ __forceinline__ double rb(int F) const { return F == 99 ? hb : A->Rb[F * A->b.fs + p]; }
 };
 
-// Writes of the generated VJP: the centre adjoint, and every D-slot adjoint
-// through the transpose of its stencil.
-struct VjpOut {
-  const AdjBlock* A;
-  long long p;
-  int i, j, k;
-  PointGates G;
-  Scatter S;
-
-  __device__ __forceinline__ void cb(int F, double v) const { S.add(F, i, j, k, v); }
-
-  __device__ __forceinline__ void line(int F, int d, int o, double v) const {
-    S.add(F, i + (d == 0 ? o : 0), j + (d == 1 ? o : 0), k + (d == 2 ? o : 0), v);
-  }
-  __device__ __forceinline__ void plane(int F, int da, int oa, int db, int ob, double v) const {
-    int ii = i, jj = j, kk = k;
-    (da == 0 ? ii : da == 1 ? jj : kk) += oa;
-    (db == 0 ? ii : db == 1 ? jj : kk) += ob;
-    S.add(F, ii, jj, kk, v);
-  }
-
-  // fderivs (diff_new.f90:946-1104)
-  __device__ __forceinline__ void grad(int F, int d, double v) const {
-    const Coef<double>& C = A->C.t;
-    if (G.ord == 2) {
-      const double c = C.d12[d] * v;
-      line(F, d, -2, c); line(F, d, -1, -8.0 * c); line(F, d, 1, 8.0 * c); line(F, d, 2, -c);
-    } else if (G.ord == 1) {
-      const double c = C.d2[d] * v;
-      line(F, d, -1, -c); line(F, d, 1, c);
-    }
-  }
-  // fdderivs (diff_new.f90:1338-1528); m: xx xy xz yy yz zz
-  __device__ __forceinline__ void hess(int F, int m, double v) const {
-    const Coef<double>& C = A->C.t;
-    const int da[6] = {0, 0, 0, 1, 1, 2}, db[6] = {0, 1, 2, 1, 2, 2};
-    const int a = da[m], b = db[m];
-    if (a == b) {
-      if (G.ord == 2) {
-        const double c = C.Fdd[a] * v;
-        line(F, a, -2, -c); line(F, a, -1, 16.0 * c); line(F, a, 0, -30.0 * c);
-        line(F, a, 1, 16.0 * c); line(F, a, 2, -c);
-      } else if (G.ord == 1) {
-        const double c = C.Sdd[a] * v;
-        line(F, a, -1, c); line(F, a, 0, -2.0 * c); line(F, a, 1, c);
-      }
-    } else {
-      if (G.ord == 2) {
-        const double cf = (m == 1 ? C.Fxy : m == 2 ? C.Fxz : C.Fyz) * v;
-        const int o[4] = {-2, -1, 1, 2};
-        const double w[4] = {1.0, -8.0, 8.0, -1.0};
-        for (int x = 0; x < 4; ++x)
-          for (int y = 0; y < 4; ++y) plane(F, a, o[x], b, o[y], cf * w[x] * w[y]);
-      } else if (G.ord == 1) {
-        const double cf = (m == 1 ? C.Sxy : m == 2 ? C.Sxz : C.Syz) * v;
-        plane(F, a, -1, b, -1, cf); plane(F, a, 1, b, -1, -cf);
-        plane(F, a, -1, b, 1, -cf); plane(F, a, 1, b, 1, cf);
-      }
-    }
-  }
-  // upwinded advection (lopsidediff.f90:321-481) and KO (kodiss.f90:190-207)
-  __device__ __forceinline__ void adv(int F, double v) const {
-    const Coef<double>& C = A->C.t;
-    const int id[3] = {i, j, k};
-    if (G.lop) {
-      for (int d = 0; d < 3; ++d) {
-        const double b = S.get(F_BETAX + d, i, j, k);
-        if (b == 0.0) continue;
-        // weights w[o + 3], o = -3 .. 3, of the branch the forward takes
-        double w[7] = {0, 0, 0, 0, 0, 0, 0};
-        const int idx = id[d], lo = G.lo3[d], hi = G.hi[d];
-        bool any = true;
-        auto up = [&](double s) { w[2] += -3 * s; w[3] += -10 * s; w[4] += 18 * s; w[5] += -6 * s; w[6] += s; };
-        auto cen = [&](double s) { w[1] += s; w[2] += -8 * s; w[4] += 8 * s; w[5] += -s; };
-        auto dn = [&](double s) { w[4] += -3 * s; w[3] += -10 * s; w[2] += 18 * s; w[1] += -6 * s; w[0] += s; };
-        if (b > 0) {
-          if (idx + 3 <= hi) up(1);
-          else if (idx + 2 <= hi) cen(1);
-          else if (idx + 1 <= hi) dn(-1);
-          else any = false;
-        } else {
-          if (idx - 3 >= lo) dn(-1);
-          else if (idx - 2 >= lo) cen(1);
-          else if (idx - 1 >= lo) up(1);
-          else any = false;
-        }
-        if (!any) continue;
-        const double bd = b * C.d12[d];
-        double u = 0.0;
-        for (int o = -3; o <= 3; ++o) {
-          if (w[o + 3] == 0.0) continue;
-          line(F, d, o, v * bd * w[o + 3]);
-          u += w[o + 3] * S.get(F, i + (d == 0 ? o : 0), j + (d == 1 ? o : 0), k + (d == 2 ? o : 0));
-        }
-        S.add(F_BETAX + d, i, j, k, v * C.d12[d] * u);   // the shift as the advecting velocity
-      }
-    }
-    if (G.ko) {
-      const double w[7] = {1, -6, 15, -20, 15, -6, 1};
-      for (int d = 0; d < 3; ++d) {
-        const double c = C.ko / C.h[d] * v;
-        for (int o = -3; o <= 3; ++o) line(F, d, o, c * w[o + 3]);
-      }
-    }
-  }
-
-  __device__ __forceinline__ void db(int s, double v) const {
-    const int F = slot_field(s), c = s - doff(F), n = dslots(F);
-    if (c == n - 1) adv(F, v);
-    else if (c < 3) grad(F, c, v);
-    else hess(F, c - 3, v);
-  }
-};
-
-// Writes of the generated VJP: the centre adjoint (added at the point) and the
-// D-slot adjoints (stored, then scattered by k_stencil_vjp).
+// Writes of the generated VJP: the centre adjoints (each written once, at the
+// point) and the D-slot adjoints (stored, then gathered by k_stencil_gather).
 struct VjpStore {
   const AdjBlock* A;
   double* Db;   // D-slot adjoints, same layout as D
   long long p;
-  __device__ __forceinline__ void cb(int F, double v) const { atomicAdd(A->Xb + F * A->b.fs + p, v); }
+  __device__ __forceinline__ void cb(int F, double v) const { A->Xb[F * A->b.fs + p] = v; }
   __device__ __forceinline__ void db(int s, double v) const { Db[s * A->dfs + p] = v; }
 };
 
@@ -211,37 +97,242 @@ __device__ __forceinline__ bool on_face_point(const BlockView& b, int i, int j, 
 }
 
 // Pointwise VJP of the right-hand side at the interior (non-face) points:
-// centre adjoints into Xb, D-slot adjoints into Db.  Db must start at zero
-// (face points leave their slots untouched).
+// centre adjoints into Xb, D-slot adjoints into Db.  Every point's Xb and Db
+// are written (zero where the right-hand side does not read the value, and
+// everywhere at face points, whose right-hand side is the Sommerfeld rule), so
+// neither needs clearing first.
 __global__ void __launch_bounds__(128) k_rhs_vjp(const AdjBlock* __restrict__ blocks, double* Db) {
   const AdjBlock& A = blocks[blockIdx.y];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < A.npts;
        p += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
     point_ijk(p, A.b.ex, i, j, k);
-    if (on_face_point(A.b, i, j, k)) continue;
+    if (on_face_point(A.b, i, j, k)) {
+      for (int F = 0; F < NFIELDS_BSSN; ++F) A.Xb[F * A.b.fs + p] = 0.0;
+      for (int s = 0; s < D_SLOTS; ++s) Db[s * A.dfs + p] = 0.0;
+      continue;
+    }
     VjpIn in{&A, p, 0.0};
     VjpStore out{&A, Db, p};
     rhs_vjp_bssn<double>(in, out);
+#pragma unroll
+    for (int F = 0; F < NFIELDS_BSSN; ++F)
+      if (!((rhs_vjp_bssn_cb_mask >> F) & 1)) A.Xb[F * A.b.fs + p] = 0.0;
   }
 }
 
-// Transpose of the stencil pass: every D-slot adjoint at a point scattered onto
-// the field values its stencil read (nslots of the layout: 135 BSSN).
-__global__ void __launch_bounds__(128) k_stencil_vjp(const AdjBlock* __restrict__ blocks, const double* Db,
-                                                     int nslots) {
-  const AdjBlock& A = blocks[blockIdx.y];
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < A.npts;
-       p += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    point_ijk(p, A.b.ex, i, j, k);
-    if (on_face_point(A.b, i, j, k)) continue;
-    VjpOut out{&A, p, i, j, k, point_gates(A.b, i, j, k), Scatter{&A}};
-#pragma unroll 1
-    for (int s = 0; s < nslots; ++s) {
-      const double v = Db[s * A.dfs + p];
-      if (v != 0.0) out.db(s, v);
+// ---------------------------------------------------------------------------
+// Transpose of the stencil pass, in gather form.
+//
+// The stencil pass computes, at every point q, D_s(q) = sum_o w_s(q, o) f(q + o)
+// with weights that depend on q only through its gates (derivative order, KO,
+// lopsided branch) and, for the advection, on the sign and value of beta(q).
+// Its transpose is gathered per target point p:
+//   fb(p) = sum_s sum_o Db_s(p - o) w_s(p - o, o),
+// so every thread owns its output point and no atomics are needed.  The
+// offsets are the ones the forward reads: lines o e_d, |o| <= 3 (gradient,
+// diagonal Hessian, upwind advection, KO) and planes (oa e_a + ob e_b),
+// oa, ob in {-2, -1, 1, 2} (mixed Hessian).  The advection also gives the
+// shift an adjoint at p itself: betab_d(p) = sum_f advb_f(p) d12_d u_f,d(p),
+// u the unweighted upwind derivative the forward used.  Blocks without
+// symmetry planes only (no mirrored reads).
+
+// Upwind weights at offsets -3..3 of the lopsided branches (lopsidediff.f90:
+// 321-481): up, centred, and the downwind stencil with the sign the forward
+// applies to it.
+__device__ __forceinline__ double lop_w(int code, int o) {
+  // o is a compile-time constant in every unrolled caller: selects, not a table
+  const double up = o == -1 ? -3.0 : o == 0 ? -10.0 : o == 1 ? 18.0 : o == 2 ? -6.0 : o == 3 ? 1.0 : 0.0;
+  const double cen = o == -2 ? 1.0 : o == -1 ? -8.0 : o == 1 ? 8.0 : o == 2 ? -1.0 : 0.0;
+  const double dn = o == -3 ? -1.0 : o == -2 ? 6.0 : o == -1 ? -18.0 : o == 0 ? 10.0 : o == 1 ? 3.0 : 0.0;
+  return code == 0 ? up : code == 1 ? cen : code == 2 ? dn : 0.0;
+}
+// branch of a point with index x along a direction (lo = imin, hi = imax) for
+// a shift component of sign b > 0 / b < 0
+__device__ __forceinline__ int lop_code(bool pos, int x, int lo, int hi) {
+  if (pos) return x + 3 <= hi ? 0 : (x + 2 <= hi ? 1 : (x + 1 <= hi ? 2 : 3));
+  return x - 3 >= lo ? 2 : (x - 2 >= lo ? 1 : (x - 1 >= lo ? 0 : 3));
+}
+
+// Per-direction fit flags of one index: bit0 +-2 fits (4th order), bit1 +-1
+// fits (2nd order), bit2 +-3 fits (KO), bit3 x <= hi - 1 (lopsided loop).
+__device__ __forceinline__ int fit_bits(int x, int hi) {
+  return ((x - 2 >= 0 && x + 2 <= hi) ? 1 : 0) | ((x - 1 >= 0 && x + 1 <= hi) ? 2 : 0) |
+         ((x - 3 >= 0 && x + 3 <= hi) ? 4 : 0) | ((x <= hi - 1) ? 8 : 0);
+}
+__device__ __forceinline__ int ord_of(int f) { return (f & 1) ? 2 : ((f & 2) ? 1 : 0); }
+
+struct GatherPt {
+  const AdjBlock* A;
+  const double* Db;   // slot 0 at this point: slot s at Db[s * dfs], neighbours at int offsets
+  const double* beta; // beta^x at this point (field stride fs)
+  int dfs, fs;
+  int id[3];
+  int str[3];
+  int fb[3];   // fit bits of p's own indices
+  __device__ __forceinline__ double db(int s, int off) const { return __ldg(Db + s * dfs + off); }
+};
+
+// Contribution to fb(p) of every slot of field F (KIND: 0 gradient + Hessian
+// + adv, 1 gradient + adv, 2 adv only); slot base `s0`.  FAST: p is at least 6
+// cells from every face, so every point its transpose reads has full gates.
+template <int KIND, bool FAST>
+__device__ __forceinline__ double gather_field(const GatherPt& g, int s0) {
+  const Coef<double>& C = g.A->C.t;
+  const BlockView& b = g.A->b;
+  const int nsl = KIND == 0 ? 10 : (KIND == 1 ? 4 : 1);
+  const int sadv = s0 + nsl - 1;
+  double acc = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    const int other = FAST ? 15 : (g.fb[d1] & g.fb[d2]);
+    const int hi = b.ex[d] - 1;
+    const double kod = C.ko / C.h[d], lpd = C.d12[d];
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      const int x = g.id[d] - o;
+      if (!FAST && (x < 0 || x > hi)) continue;
+      const int q = -o * g.str[d];
+      const int f = FAST ? 15 : (other & fit_bits(x, hi));
+      if (KIND != 2 && o >= -2 && o <= 2) {
+        const int ord = FAST ? 2 : ord_of(f);
+        const double w4 = o == -2 ? 1.0 : o == -1 ? -8.0 : o == 1 ? 8.0 : o == 2 ? -1.0 : 0.0;
+        const double w2 = o == -1 ? -1.0 : o == 1 ? 1.0 : 0.0;
+        if (o != 0) {
+          const double wg = ord == 2 ? C.d12[d] * w4 : (ord == 1 ? C.d2[d] * w2 : 0.0);
+          acc += g.db(s0 + d, q) * wg;
+        }
+        if (KIND == 0) {
+          const double h4 = o == 0 ? -30.0 : (o == -1 || o == 1) ? 16.0 : -1.0;
+          const double h2 = o == 0 ? -2.0 : (o == -1 || o == 1) ? 1.0 : 0.0;
+          const int sh = s0 + 3 + (d == 0 ? 0 : d == 1 ? 3 : 5);   // xx, yy, zz
+          if (FAST || ord == 2) acc += g.db(sh, q) * (C.Fdd[d] * h4);
+          else if (ord == 1 && o >= -1 && o <= 1) acc += g.db(sh, q) * (C.Sdd[d] * h2);
+        }
+      }
+      const double ab = g.db(sadv, q);
+      const double wko = o == 0 ? -20.0 : (o == 1 || o == -1) ? 15.0 : (o == 2 || o == -2) ? -6.0 : 1.0;
+      double w = (f & 4) ? kod * wko : 0.0;
+      if (f & 8) {
+        const double bq = __ldg(g.beta + d * g.fs + q);
+        const int code = FAST ? (bq > 0.0 ? 0 : 2) : lop_code(bq > 0.0, x, 0, hi);
+        w += bq * lpd * lop_w(code, o);   // zero where beta vanishes
+      }
+      acc += ab * w;
     }
+  }
+  if (KIND == 0) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {   // xy, xz, yz
+      const int a = m == 2 ? 1 : 0, c = m == 0 ? 1 : 2, e = 3 - a - c;
+      const int sm = s0 + 3 + (m == 0 ? 1 : m == 1 ? 2 : 4);
+      const double F4 = m == 0 ? C.Fxy : m == 1 ? C.Fxz : C.Fyz;
+      const double S2 = m == 0 ? C.Sxy : m == 1 ? C.Sxz : C.Syz;
+      const int ha = b.ex[a] - 1, hc = b.ex[c] - 1;
+#pragma unroll
+      for (int oa = -2; oa <= 2; ++oa) {
+        if (oa == 0) continue;
+        const int xa = g.id[a] - oa;
+        if (!FAST && (xa < 0 || xa > ha)) continue;
+        const int fa = FAST ? 15 : (fit_bits(xa, ha) & g.fb[e]);
+        const double wa = oa == -2 ? 1.0 : oa == -1 ? -8.0 : oa == 1 ? 8.0 : -1.0;
+        double row = 0.0;   // FAST: the 4th-order taps of this oa summed over oc first
+#pragma unroll
+        for (int oc = -2; oc <= 2; ++oc) {
+          if (oc == 0) continue;
+          const int xc = g.id[c] - oc;
+          if (!FAST && (xc < 0 || xc > hc)) continue;
+          const double wc = oc == -2 ? 1.0 : oc == -1 ? -8.0 : oc == 1 ? 8.0 : -1.0;
+          const double v = g.db(sm, -oa * g.str[a] - oc * g.str[c]);
+          if (FAST) {
+            row += wc * v;
+          } else {
+            const int ord = ord_of(fa & fit_bits(xc, hc));
+            if (ord == 2) acc += v * (F4 * wa * wc);
+            else if (ord == 1 && oa * oa == 1 && oc * oc == 1) acc += v * (S2 * (double)(oa * oc));
+          }
+        }
+        if (FAST) acc += row * (F4 * wa);
+      }
+    }
+  }
+  return acc;
+}
+
+// Xb_F += transpose(stencil pass)(Db) of field F = blockIdx.y at every point
+// (BSSN layout, 135 slots); one thread per (point, field).  Offsets are 32-bit
+// (amss_adjoint_create bounds D_SLOTS x the field stride).
+__global__ void __launch_bounds__(128) k_stencil_gather(const AdjBlock* __restrict__ A, const double* __restrict__ Db) {
+  const BlockView& b = A->b;
+  const int F = blockIdx.y;
+  const int s0 = doff(F), n = dslots(F);
+  const int npts = (int)A->npts;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += gridDim.x * blockDim.x) {
+    GatherPt g;
+    g.A = A;
+    g.Db = Db + p;
+    g.beta = A->X + F_BETAX * b.fs + p;
+    g.dfs = (int)A->dfs;
+    g.fs = (int)b.fs;
+    g.id[0] = p % b.ex[0];
+    g.id[1] = (p / b.ex[0]) % b.ex[1];
+    g.id[2] = p / (b.ex[0] * b.ex[1]);
+    g.str[0] = 1;
+    g.str[1] = b.ex[0];
+    g.str[2] = b.ex[0] * b.ex[1];
+    bool fast = true;
+    for (int d = 0; d < 3; ++d) {
+      g.fb[d] = fit_bits(g.id[d], b.ex[d] - 1);
+      fast = fast && g.id[d] >= 6 && g.id[d] <= b.ex[d] - 7;
+    }
+    double acc;
+    if (n == 10) acc = fast ? gather_field<0, true>(g, s0) : gather_field<0, false>(g, s0);
+    else if (n == 4) acc = fast ? gather_field<1, true>(g, s0) : gather_field<1, false>(g, s0);
+    else acc = fast ? gather_field<2, true>(g, s0) : gather_field<2, false>(g, s0);
+    A->Xb[F * b.fs + p] += acc;
+  }
+}
+
+// The shift as the advecting velocity: betab_d(p) += sum_F advb_F(p) d12_d
+// sum_o w_o f_F(p + o e_d), w the upwind weights the forward used at p
+// (lopsidediff.f90:321-481).
+__global__ void __launch_bounds__(128) k_beta_adjoint(const AdjBlock* __restrict__ A, const double* __restrict__ Db) {
+  const BlockView& b = A->b;
+  const Coef<double>& C = A->C.t;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < A->npts;
+       p += (long long)gridDim.x * blockDim.x) {
+    int id[3];
+    point_ijk(p, b.ex, id[0], id[1], id[2]);
+    const long long str[3] = {1, b.ex[0], (long long)b.ex[0] * b.ex[1]};
+    if (!(fit_bits(id[0], b.ex[0] - 1) & fit_bits(id[1], b.ex[1] - 1) & fit_bits(id[2], b.ex[2] - 1) & 8)) continue;
+    int code[3];
+    bool any = false;
+    for (int d = 0; d < 3; ++d) {
+      const double bq = A->X[(F_BETAX + d) * b.fs + p];
+      code[d] = bq == 0.0 ? 3 : lop_code(bq > 0.0, id[d], 0, b.ex[d] - 1);
+      any = any || code[d] != 3;
+    }
+    if (!any) continue;
+    double bb[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int F = 0; F < NFIELDS_BSSN; ++F) {
+      const double ab = Db[(doff(F) + dslots(F) - 1) * A->dfs + p];
+      if (ab == 0.0) continue;
+      const double* X = A->X + F * b.fs + p;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (code[d] == 3) continue;
+        double u = 0.0;
+#pragma unroll
+        for (int o = -3; o <= 3; ++o) {
+          const double w = lop_w(code[d], o);
+          if (w != 0.0) u += w * X[o * str[d]];
+        }
+        bb[d] += ab * C.d12[d] * u;
+      }
+    }
+    for (int d = 0; d < 3; ++d) A->Xb[(F_BETAX + d) * b.fs + p] += bb[d];
   }
 }
 
@@ -314,7 +405,7 @@ __global__ void __launch_bounds__(128) k_ham_loss(const AdjBlock* __restrict__ b
 }
 
 // Pointwise VJP of sum H^2 dV (Hb = 2 H dV on the interior cells): centre
-// adjoints into Xb, D-slot adjoints into Db (scattered by k_stencil_vjp).
+// adjoints into Xb, D-slot adjoints into Db (gathered by k_stencil_gather).
 __global__ void __launch_bounds__(128) k_ham_vjp(const AdjBlock* __restrict__ blocks, int gw, double dV,
                                                  const double* H, double* Db) {
   const AdjBlock& A = blocks[blockIdx.y];
@@ -332,34 +423,69 @@ __global__ void __launch_bounds__(128) k_ham_vjp(const AdjBlock* __restrict__ bl
 
 // enforce_ga_point's VJP: adjoint of the metric / A~ components of Z (pre-
 // enforce values, offsets) given the adjoint of E(Z); other fields pass through.
+// enforce_vjp's reads: the pre-enforce metric / A~ (Z) and the adjoint of
+// E(Z), given as the sum of up to two arrays.
 struct EnfIn {
   const double* Z;
-  const double* Eb;
+  const double* E1;
+  const double* E2;
   long long fs, p;
   __device__ __forceinline__ double c(int m) const { return Z[(F_GXX + m) * fs + p]; }
   __device__ __forceinline__ double d(int) const { return 0.0; }
-  __device__ __forceinline__ double rb(int m) const { return Eb[(F_GXX + m) * fs + p]; }
+  __device__ __forceinline__ double rb(int m) const {
+    const long long o = (F_GXX + m) * fs + p;
+    return E2 ? E1[o] + E2[o] : E1[o];
+  }
 };
 struct EnfOut {
-  double* Zb;
-  long long fs, p;
-  __device__ __forceinline__ void cb(int m, double v) { Zb[(F_GXX + m) * fs + p] = v; }
+  double zb[12];
+  __device__ __forceinline__ void cb(int m, double v) { zb[m] = v; }
   __device__ __forceinline__ void db(int, double) {}
 };
 
-// Zb = mask(Z) * E'(Z)^T Eb (chi masked where the floor held Z at chitiny).
-__global__ void __launch_bounds__(128) k_enforce_vjp(const double* __restrict__ Z, const double* __restrict__ Eb,
-                                                     double* __restrict__ Zb, long long n, long long fs,
-                                                     double chitiny, int enforce) {
+// The reverse of one enforce + chi floor, fused with what consumes its
+// result: Zb = mask(Z) E'(Z)^T (E1 + E2) per point (chi masked where the floor
+// held Z at chitiny; E2 may be null), then
+//   out = Zb (if out), acc0 += Zb (if acc0), acc1 += c1 Zb (if acc1).
+__global__ void __launch_bounds__(128) k_enforce_vjp(const double* __restrict__ Z, const double* E1,
+                                                     const double* E2, double* out, double* acc0, double* acc1,
+                                                     double c1, long long n, long long fs, double chitiny) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    for (int f = 0; f < NFIELDS_BSSN; ++f)
-      if (!enforce || f < F_GXX || f > F_AZZ) Zb[f * fs + p] = Eb[f * fs + p];
-    if (enforce) {
-      EnfIn in{Z, Eb, fs, p};
-      EnfOut out{Zb, fs, p};
-      enforce_vjp<double>(in, out);
+    EnfIn in{Z, E1, E2, fs, p};
+    EnfOut eo;
+    enforce_vjp<double>(in, eo);
+    const bool floor_held = Z[F_CHI * fs + p] == chitiny;
+#pragma unroll
+    for (int f = 0; f < NFIELDS_BSSN; ++f) {
+      const long long o = f * fs + p;
+      double v;
+      if (f >= F_GXX && f <= F_AZZ) v = eo.zb[f - F_GXX];
+      else v = E2 ? E1[o] + E2[o] : E1[o];
+      if (f == F_CHI && floor_held) v = 0.0;
+      if (out) out[o] = v;
+      if (acc0) acc0[o] += v;
+      if (acc1) acc1[o] += c1 * v;
     }
-    if (Z[F_CHI * fs + p] == chitiny) Zb[F_CHI * fs + p] = 0.0;
+  }
+}
+
+// Seed of one step's reverse: with Yb = mask(U_new) Ub,
+//   U0b = Yb, R3b = R0b = dt/6 Yb, R1b = R2b = dt/3 Yb.
+__global__ void __launch_bounds__(128) k_step_seed(const double* __restrict__ Ub, const double* __restrict__ Unew,
+                                                   double* U0b, double* R0b, double* R1b, double* R2b, double* R3b,
+                                                   double dt, long long n, long long fs, double chitiny) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const bool floor_held = Unew[F_CHI * fs + p] == chitiny;
+#pragma unroll 4
+    for (int f = 0; f < NFIELDS_BSSN; ++f) {
+      const long long o = f * fs + p;
+      const double y = (f == F_CHI && floor_held) ? 0.0 : Ub[o];
+      U0b[o] = y;
+      R0b[o] = (dt / 6.0) * y;
+      R3b[o] = (dt / 6.0) * y;
+      R1b[o] = (dt / 3.0) * y;
+      R2b[o] = (dt / 3.0) * y;
+    }
   }
 }
 

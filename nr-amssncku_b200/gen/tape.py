@@ -222,6 +222,9 @@ def emit_vjp(tape, name):
         if i in defined:
             w(f"  out.db({s}, a{i});")
     w("}")
+    mask = sum(1 << f for f, i in tape.inputs_c.items() if i in defined)
+    w(f"// centre fields whose adjoint {name} writes (bit F)")
+    w(f"constexpr unsigned long long {name}_cb_mask = 0x{mask:x}ull;")
     return "\n".join(L) + "\n"
 
 
