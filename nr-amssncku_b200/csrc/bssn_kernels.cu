@@ -140,6 +140,12 @@ Coef<T> make_coef(const double dx[3], double eps) {
     c.Fdd[d] = (T)(F1o12 / (dx[d] * dx[d]));
     c.Sdd[d] = (T)(ONE / (dx[d] * dx[d]));
     c.h[d] = (T)dx[d];
+    c.hinv[d] = (T)(ONE / dx[d]);
+  }
+  c.hpow2 = 1;
+  for (int d = 0; d < 3; ++d) {
+    int e;
+    if (!(dx[d] > 0.0) || std::frexp(dx[d], &e) != 0.5) c.hpow2 = 0;
   }
   c.Fxy = (T)(F1o144 / (dx[0] * dx[1]));
   c.Fxz = (T)(F1o144 / (dx[0] * dx[2]));

@@ -78,8 +78,8 @@ __device__ __forceinline__ void finish_field(const P& q, const Coefs<T>& C, cons
       auto kx = [&](int o) { return q.template v<A, F>(o, 0, 0); };
       auto ky = [&](int o) { return q.template v<A, F>(0, o, 0); };
       auto kz = [&](int o) { return q.template v<A, F>(0, 0, o); };
-      const A ks = divh(ko_sum_rn<A, KO1>(kx), c.h[0]) + divh(ko_sum_rn<A, KO1>(ky), c.h[1]) +
-                   divh(ko_sum_rn<A, KO1>(kz), c.h[2]);
+      const A ks = kodiv(ko_sum_rn<A, KO1>(kx), c, 0) + kodiv(ko_sum_rn<A, KO1>(ky), c, 1) +
+                   kodiv(ko_sum_rn<A, KO1>(kz), c, 2);
       r = r + (T)(c.ko * ks);
     }
     epi.template put<F>(r);

@@ -130,6 +130,15 @@ struct PlaneFetch {
 template <typename A, typename FN>
 __device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, int hi) {
   const A F3 = A(3), F10 = A(10), F18 = A(18), F6 = A(6), EIT = A(8);
+  if (idx - 3 >= lo && idx + 3 <= hi) {
+    // both full-width branches fit: the same arithmetic on the mirrored line,
+    // chosen by selects instead of divergent branches
+    const bool pos = b > A(0);
+    const A fa = pos ? f(-1) : f(1), fb = f(0), fc = pos ? f(1) : f(-1);
+    const A fd = pos ? f(2) : f(-2), fe = pos ? f(3) : f(-3);
+    const A s = -F3 * fa - F10 * fb + F18 * fc - F6 * fd + fe;
+    return pos ? bd * s : (b < A(0) ? -bd * s : A(0));
+  }
   A d = A(0);
   if (b > A(0)) {
     if (idx + 3 <= hi) d = bd * (-F3 * f(-1) - F10 * f(0) + F18 * f(1) - F6 * f(2) + f(3));
@@ -285,11 +294,11 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
         const bool ko1 = B.nf == NFIELDS_Z4C && (F == F_GXX || F == F_GYY || F == F_GZZ);
         A ks;
         if (ko1)
-          ks = divh(ko_sum_rn<A, true>(X), C.h[0]) + divh(ko_sum_rn<A, true>(Y), C.h[1]) +
-               divh(ko_sum_rn<A, true>(Z), C.h[2]);
+          ks = kodiv(ko_sum_rn<A, true>(X), C, 0) + kodiv(ko_sum_rn<A, true>(Y), C, 1) +
+               kodiv(ko_sum_rn<A, true>(Z), C, 2);
         else
-          ks = divh(ko_sum_rn<A, false>(X), C.h[0]) + divh(ko_sum_rn<A, false>(Y), C.h[1]) +
-               divh(ko_sum_rn<A, false>(Z), C.h[2]);
+          ks = kodiv(ko_sum_rn<A, false>(X), C, 0) + kodiv(ko_sum_rn<A, false>(Y), C, 1) +
+               kodiv(ko_sum_rn<A, false>(Z), C, 2);
         adv = adv + C.ko * ks;
       }
       d[(o + dslots(F) - 1) * dfs + p] = (T)adv;

@@ -24,6 +24,8 @@ struct Coef {
   T Fxy, Fxz, Fyz;   // (1/144)/(dx*dy)
   T Sxy, Sxz, Syz;   // 0.25/(dx*dy)
   T h[3];            // dx itself (KO divides by it)
+  T hinv[3];         // 1/dx, used instead of the division when every dx is a power of two (exact)
+  int hpow2;
   T ko;              // eps/64
 };
 
@@ -321,9 +323,10 @@ __device__ __forceinline__ T ko_sum_rn(const FN& f) {
 }
 
 template <typename T>
-__device__ __forceinline__ T divh(T a, T h) {
-  if constexpr (sizeof(T) == 8) return a / h;   // the reference divides
-  else return a * (T(1) / h);
+__device__ __forceinline__ T kodiv(T a, const Coef<T>& c, int d) {
+  // the reference divides by dx; for dx = 2^k the product with 2^-k is the same number
+  if constexpr (sizeof(T) == 8) return c.hpow2 ? a * c.hinv[d] : a / c.h[d];
+  else return a * (T(1) / c.h[d]);
 }
 
 }  // namespace amss

@@ -7,6 +7,9 @@
 #ifndef AMSS_SUBSTEP_MINB   // resident CTAs of 128 threads the register-pass kernel is compiled for
 #define AMSS_SUBSTEP_MINB 2
 #endif
+#ifndef AMSS_SUBSTEP_MINB_F32   // the same for FP32 arithmetic (fits 168 registers without spills)
+#define AMSS_SUBSTEP_MINB_F32 3
+#endif
 #ifndef AMSS_POINTWISE_PREFETCH   // L2 prefetch of the next tile's rows in the register pass
 #define AMSS_POINTWISE_PREFETCH 0
 #endif
@@ -18,7 +21,7 @@ namespace amss {
 // SPLIT: the stencil terms come from the D array the stencil pass (k_deriv)
 // wrote for this substep; otherwise every stencil is evaluated here.
 template <typename T, typename SI, typename SO, bool SYMM, bool SPLIT, bool Z4C>
-__global__ void __launch_bounds__(128, AMSS_SUBSTEP_MINB) k_substep(const StepBlock<T>* __restrict__ blocks,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : AMSS_SUBSTEP_MINB) k_substep(const StepBlock<T>* __restrict__ blocks,
                                                                     const int2* __restrict__ tiles, int ntiles,
                                                                     int sub, RKConst rk, int enforce,
                                                                     unsigned* status, const T* __restrict__ D,
