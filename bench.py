@@ -2,7 +2,8 @@
 """Throughput of the BSSN RK4 evolution step on B200 (zone-updates/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-                    [--workload amr|single64] [--kernel split|fused] [--impl ours|reference]
+                    [--workload amr|amr8|singleN|adjoint96] [--formulation bssn|z4c]
+                    [--kernel split|fused] [--impl ours|reference] [--report mixed]
 
 A step is one Berger-Oliger coarse step of the workload (every level
 advanced to the next coarse time, with its AMR transfers).
@@ -11,6 +12,11 @@ CUDA events on the engine's stream; `e2e` is the same metric through the
 public engine API with the state copied in from pinned host memory and back out
 every step.  Under torchrun each rank advances its own copy of the workload
 (no data-path collective); the step time is the max over ranks.
+
+--workload adjoint96 prints the adjoint step time over the forward step time
+of the 96^3 gradient workload instead; --report mixed prints the mixed form's
+field and constraint errors against FP64 after 20 coarse steps of the amr
+hierarchy with m = 0.6, 0.4 and noise 1e-6.
 
 --impl reference times the CPU restatement of the reference's Fortran path
 (oracle/, the reference itself cannot be compiled in this image) on the host
@@ -60,6 +66,11 @@ def workload(name):
                     desc="96^3 coarse on [-48,48]^3 + 7 box-in-box levels of 64^3 cells around BL m=1 at "
                          "(0.1,0.05,0.02), blocks 48-160 cells, dt0=0.25 dx0, noise 1e-8; step = one "
                          "Berger-Oliger coarse step")
+    if name == "amr3":
+        H = box_in_box(96, 48.0, [(-3.0, 0.0, 0.0), (3.0, 0.0, 0.0)], 7, box_cells=48, seed=1,
+                       block_min=18, block_max=74)
+        return dict(H=H, masses=[0.6, 0.4], pos=[[-3.0, 0.0, 0.0], [3.0, 0.0, 0.0]], noise=1e-6, eps=0.1,
+                    courant=0.25, desc="the amr hierarchy with BL m=0.6, 0.4 at (+-3,0,0) and noise 1e-6")
     if name.startswith("single") and name[6:].isdigit():
         n = int(name[6:])
         H = single_block(n, -n / 8.0, n / 8.0, 3)
@@ -393,6 +404,73 @@ def run_adjoint(args):
     }
 
 
+def constraint_l2(H, states, eps):
+    """Per level: L2 norms sqrt(sum f^2 h^3) of the Hamiltonian constraint and of
+    the momentum constraint magnitude over the cells each block owns inside its
+    patch's physical box (Parallel::L2Norm with l2normhelper; buffer cells,
+    filled by prolongation, and ghost cells excluded), from compute_rhs_bssn_
+    with co = 0 (FP64) on every block."""
+    from amss_b200 import dropin
+    nlev = len(H.levels)
+    ham = [0.0] * nlev
+    mom = [0.0] * nlev
+    for bi, b in enumerate(H.blocks):
+        p = H.levels[b.level][b.patch]
+        X, Y, Z = H.coords(b)
+        st = np.ascontiguousarray(states[bi][:24])
+        cons = dropin.compute_rhs_bssn(X, Y, Z, st, eps=eps, co=0)[4]
+        lo = [max(b.own_lo[d], p.lo[d]) - b.org[d] for d in range(3)]
+        hi = [min(b.own_hi[d], p.hi[d]) - b.org[d] for d in range(3)]
+        if any(hi[d] <= lo[d] for d in range(3)):
+            continue
+        sl = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+        dv = H.h(b.level) ** 3
+        ham[b.level] += float(np.sum(cons[0][sl] ** 2)) * dv
+        mom[b.level] += float(np.sum(cons[1][sl] ** 2 + cons[2][sl] ** 2 + cons[3][sl] ** 2)) * dv
+    return [float(np.sqrt(v)) for v in ham], [float(np.sqrt(v)) for v in mom]
+
+
+def run_mixed_report(args):
+    """amr3 (m = 0.6, 0.4, noise 1e-6): the mixed form against the FP64 form
+    after `--report-steps` coarse steps from the same initial state: relative
+    max-norm error of every field over all blocks, and per-level constraint L2
+    norms of both."""
+    import torch
+    import amss_b200
+    from amss_b200.dropin import STATE_NAMES
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    w = workload("amr3")
+    H = w["H"]
+    init = make_initial(w)
+    dt0 = w["courant"] * H.h0
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng = amss_b200.Engine.from_hierarchy(H, precision=prec, eps=w["eps"])
+        for i, st in enumerate(init):
+            eng.set_state(i, st)
+        eng.run_coarse_graph(dt0, args.report_steps, 1)
+        if eng.sync():
+            raise SystemExit(f"{prec}: NaN in the state")
+        out[prec] = [eng.get_state(i) for i in range(len(H.blocks))]
+        eng.close()
+    err = {}
+    for f, name in enumerate(STATE_NAMES):
+        num = max(float(np.max(np.abs(m[f] - r[f]))) for m, r in zip(out["mixed"], out["fp64"]))
+        den = max(float(np.max(np.abs(r[f]))) for r in out["fp64"])
+        err[name] = num / den if den > 0 else num
+    h64, m64 = constraint_l2(H, out["fp64"], w["eps"])
+    hmx, mmx = constraint_l2(H, out["mixed"], w["eps"])
+    return {
+        "metric": f"mixed vs FP64 after {args.report_steps} coarse steps: relative max-norm field error, "
+                  "constraint L2 norms per level",
+        "value": max(err.values()), "unit": "relative max-norm error (worst field)", "higher_is_better": False,
+        "n_gpus": 1, "dtype": "f32 stencils / f64 state", "data": "synthetic (Brill-Lindquist + noise 1e-6)",
+        "field_max_rel_err": err,
+        "ham_l2": {"fp64": h64, "mixed": hmx}, "mom_l2": {"fp64": m64, "mixed": mmx},
+        "config": {"workload": f"amr3: {w['desc']}", "coarse_steps": args.report_steps},
+    }
+
+
 def run_reference(args, rank, world):
     """The reference arm: the oracle (the C restatement of the reference's
     Fortran) on all host cores, one finest-level RK4 step of the workload per
@@ -449,12 +527,19 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--report", choices=["none", "mixed"], default="none",
+                    help="mixed: the mixed form's field and constraint errors against FP64 (amr3 hierarchy)")
+    ap.add_argument("--report-steps", type=int, default=20)
     ap.add_argument("--adj-n", type=int, default=96, help="adjoint96: interior cells per side (smaller for ncu)")
     ap.add_argument("--adj-steps", type=int, default=200, help="adjoint96: RK4 steps")
     ap.add_argument("--adj-ck", type=int, default=20, help="adjoint96: checkpoint interval")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.report == "mixed":
+        if rank == 0:
+            print(json.dumps(run_mixed_report(args)))
+        return
     if args.workload == "adjoint96":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}))
