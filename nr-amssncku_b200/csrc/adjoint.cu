@@ -16,7 +16,7 @@
 //   s = 3, 2, 1:  Xb_s = F'(X_s)^T R_sb;  Zb = mask(Z_{s-1}) E'(Z_{s-1})^T Xb_s;
 //                 U0b += Zb;  R_{s-1}b += c_{s-1} Zb        (c = dt/2, dt/2, dt)
 //   U0b += F'(X_0)^T R0b;  Ub(previous step) = E'(U0 raw)^T U0b.
-// F'^T is k_rhs_vjp (pointwise, generated) + k_stencil_gather (stencil
+// F'^T is k_rhs_vjp (pointwise, generated) + k_stencil_gather_tiled (stencil
 // transpose) + k_face_vjp (Sommerfeld transpose); E'^T and the floor mask are
 // k_enforce_vjp.
 #include <cmath>
@@ -93,6 +93,8 @@ struct amss_adjoint {
   std::vector<double*> ckpt;             // checkpoints
   double* seg = nullptr;                 // segment storage: per step U0raw, Z0, Z1, Z2, Unew
   int seg_cap = 0;
+  double* Dseg = nullptr;                // the segment's stencil terms, per step and substep (if HBM allows)
+  int dseg_cap = 0;
   double* Ub = nullptr;
   double* U0b = nullptr;
   double* Rb[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -133,7 +135,9 @@ int set_tables(amss_adjoint* a, double* Unew, double* Z0, double* Z1, double* Z2
 
 // One forward RK4 step: U0raw -> Unew (may alias U0raw: it is read first),
 // the pre-enforce stages into Z0..Z2.
-int fwd_step(amss_adjoint* a, const double* U0raw, double* Unew, double* Z0, double* Z1, double* Z2) {
+// Dsub: where each substep's stencil terms go (null: the scratch a->D).
+int fwd_step(amss_adjoint* a, const double* U0raw, double* Unew, double* Z0, double* Z1, double* Z2,
+             double* const* Dsub = nullptr) {
   cudaStream_t s = a->stream;
   const long long n = a->npts, fs = a->fs;
   k_enforce_copy<<<grid_of(n), 128, 0, s>>>(U0raw, a->U0, n, fs);
@@ -147,9 +151,10 @@ int fwd_step(amss_adjoint* a, const double* U0raw, double* Unew, double* Z0, dou
   rk.chitiny = a->chitiny;
   for (int sub = 0; sub < 4; ++sub) {
     const StepBlock<double>* T = a->dtab + sub;
-    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+    double* D = Dsub ? Dsub[sub] : a->D;
+    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, D, a->fs, std::min(a->nitems, 148 * 16), s)));
     AMSS_CK((launch_substep<double, double, false, true, false>(T, a->dtiles, a->ntiles, sub, rk, 0, a->dstatus,
-                                                              std::min(a->ntiles, 148 * 8), s, a->D, a->fs)));
+                                                              std::min(a->ntiles, 148 * 8), s, D, a->fs)));
     AMSS_CK((launch_face<double, double, false>(T, a->dfaces, a->nfaces, sub, rk, 0, a->dstatus, s)));
     a->launches += 3;
     if (sub < 3) {
@@ -162,17 +167,22 @@ int fwd_step(amss_adjoint* a, const double* U0raw, double* Unew, double* Z0, dou
 }
 
 // Xb = F'(X)^T Rb at the input of substep `sub` (table sub), X = input buffer.
-int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, double* Xbv) {
+// Dpre: X's stencil terms as the forward stored them, or null to recompute.
+int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, double* Xbv, const double* Dpre) {
   cudaStream_t s = a->stream;
   const StepBlock<double>* T = a->dtab + sub;
-  AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+  if (!Dpre) {
+    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+    a->launches++;
+  }
+  a->host_adj.D = Dpre ? Dpre : a->D;
   a->host_adj.X = Xin;
   a->host_adj.Rb = Rbv;
   a->host_adj.Xb = Xbv;
   AMSS_CK(cudaMemcpyAsync(a->dadj, &a->host_adj, sizeof(AdjBlock), cudaMemcpyHostToDevice, s));
   k_rhs_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, a->Db);
   AMSS_CK(cudaGetLastError());
-  k_stencil_gather<<<dim3(grid_of(a->npts), NFIELDS_BSSN), 128, 0, s>>>(a->dadj, a->Db);
+  k_stencil_gather_tiled<<<a->nitems, DTHREADS, kTgSmem, s>>>(a->dadj, a->ditems, a->Db);
   AMSS_CK(cudaGetLastError());
   k_beta_adjoint<<<grid_of(a->npts), 128, 0, s>>>(a->dadj, a->Db);
   AMSS_CK(cudaGetLastError());
@@ -181,7 +191,7 @@ int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, doub
     AMSS_CK(cudaGetLastError());
     a->launches++;
   }
-  a->launches += 4;
+  a->launches += 3;
   return 0;
 }
 
@@ -197,6 +207,11 @@ extern "C" amss_adjoint* amss_adjoint_create(const int ex[3], const double bbox[
     return nullptr;
   }
   if (check_device("amss_adjoint_create") != 0) return nullptr;
+  if (cudaFuncSetAttribute(k_stencil_gather_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTgSmem) !=
+      cudaSuccess) {
+    amss_fail(AMSS_ERR_CUDA, "amss_adjoint_create: cannot reserve shared memory for the stencil transpose");
+    return nullptr;
+  }
   amss_adjoint* a = new amss_adjoint();
   for (int d = 0; d < 3; ++d) a->ex[d] = ex[d];
   a->npts = (long long)ex[0] * ex[1] * ex[2];
@@ -296,7 +311,7 @@ extern "C" void amss_adjoint_destroy(amss_adjoint* a) {
   if (a->stream) cudaStreamSynchronize(a->stream);
   void* ptrs[] = {a->dstatus, a->dlvl, a->dcoord, a->dtab, a->dadj, a->ditems, a->dtiles, a->dfaces, a->D, a->Db,
                   a->U, a->U0, a->X[0], a->X[1], a->X[2], a->K, a->Zs, a->H, a->dloss, a->seg, a->Ub, a->U0b,
-                  a->Rb[0], a->Rb[1], a->Rb[2], a->Rb[3], a->Xb};
+                  a->Rb[0], a->Rb[1], a->Rb[2], a->Rb[3], a->Xb, a->Dseg};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (double* c : a->ckpt) cudaFree(c);
@@ -329,6 +344,7 @@ static int loss_and_grad(amss_adjoint* a, double* loss, bool want_grad) {
   a->host_tab[0].tl[0] = a->U;   // stencil pass of U (substep-0 input)
   AMSS_CK(cudaMemcpyAsync(a->dtab, a->host_tab, sizeof(StepBlock<double>), cudaMemcpyHostToDevice, s));
   AMSS_CK((launch_deriv<double, double>(a->dtab, a->ditems, a->nitems, 0, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+  a->host_adj.D = a->D;
   a->host_adj.X = a->U;
   a->host_adj.Rb = nullptr;
   a->host_adj.Xb = a->Ub;
@@ -342,7 +358,7 @@ static int loss_and_grad(amss_adjoint* a, double* loss, bool want_grad) {
     AMSS_CK(cudaMemsetAsync(a->Db, 0, (size_t)D_SLOTS * a->fs * sizeof(double), s));
     k_ham_vjp<<<dim3(grid_of(a->npts), 1), 128, 0, s>>>(a->dadj, gw, dV, a->H, a->Db);
     AMSS_CK(cudaGetLastError());
-    k_stencil_gather<<<dim3(grid_of(a->npts), NFIELDS_BSSN), 128, 0, s>>>(a->dadj, a->Db);   // H reads no adv slot
+    k_stencil_gather_tiled<<<a->nitems, DTHREADS, kTgSmem, s>>>(a->dadj, a->ditems, a->Db);   // H reads no adv slot
     AMSS_CK(cudaGetLastError());
     a->launches += 2;
   }
@@ -358,9 +374,11 @@ extern "C" int amss_adjoint_forward(amss_adjoint* a, double dt, int nsteps, int 
   a->ck = ck;
   const size_t sb = state_bytes(a);
   const int nck = (nsteps + ck - 1) / ck;
-  for (double* c : a->ckpt) cudaFree(c);
-  a->ckpt.assign(nck + 1, nullptr);   // + the final state
-  for (int m = 0; m <= nck; ++m) AMSS_CK(cudaMalloc(&a->ckpt[m], sb));
+  if ((int)a->ckpt.size() != nck + 1) {   // + the final state; kept across calls of the same length
+    for (double* c : a->ckpt) cudaFree(c);
+    a->ckpt.assign(nck + 1, nullptr);
+    for (int m = 0; m <= nck; ++m) AMSS_CK(cudaMalloc(&a->ckpt[m], sb));
+  }
   cudaStream_t s = a->stream;
   double* Zs1 = a->Zs + (size_t)NFIELDS_BSSN * a->fs;
   double* Zs2 = a->Zs + (size_t)2 * NFIELDS_BSSN * a->fs;
@@ -390,6 +408,23 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
     a->seg_cap = need;
   }
   auto st = [&](int slot) { return a->seg + (size_t)slot * m; };
+  // The stencil terms of every substep of a segment (4 ck arrays of D_SLOTS
+  // fields; 92 GB at 96^3 + ghosts with ck = 20) are kept when the device has
+  // room for them, so the reverse sweep reads them instead of recomputing them.
+  const size_t dsz = (size_t)D_SLOTS * fs;
+  if (a->dseg_cap < 4 * a->ck) {
+    if (a->Dseg) cudaFree(a->Dseg);
+    a->Dseg = nullptr;
+    a->dseg_cap = 0;
+    size_t free_b = 0, total_b = 0;
+    const size_t want = (size_t)4 * a->ck * dsz * sizeof(double);
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b > want + ((size_t)4 << 30) &&
+        cudaMalloc(&a->Dseg, want) == cudaSuccess)
+      a->dseg_cap = 4 * a->ck;
+    else
+      (void)cudaGetLastError();   // not enough room: recompute instead
+  }
+  auto dst = [&](int t, int sub) { return a->Dseg ? a->Dseg + (size_t)(4 * t + sub) * dsz : nullptr; };
   // dL/dU at the final time
   double loss = 0;
   AMSS_CK(cudaMemcpyAsync(a->U, a->ckpt[nck], sb, cudaMemcpyDeviceToDevice, s));
@@ -401,7 +436,9 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
     AMSS_CK(cudaMemcpyAsync(a->U, a->ckpt[sg], sb, cudaMemcpyDeviceToDevice, s));
     for (int t = 0; t < ns; ++t) {
       AMSS_CK(cudaMemcpyAsync(st(4 * t), a->U, sb, cudaMemcpyDeviceToDevice, s));
-      if (int rc = fwd_step(a, a->U, a->U, st(4 * t + 1), st(4 * t + 2), st(4 * t + 3))) return rc;
+      double* const dts[4] = {dst(t, 0), dst(t, 1), dst(t, 2), dst(t, 3)};
+      if (int rc = fwd_step(a, a->U, a->U, st(4 * t + 1), st(4 * t + 2), st(4 * t + 3), a->Dseg ? dts : nullptr))
+        return rc;
     }
     AMSS_CK(cudaMemcpyAsync(st(4 * ns), a->U, sb, cudaMemcpyDeviceToDevice, s));
     for (int t = ns - 1; t >= 0; --t) {
@@ -420,12 +457,12 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
       // substeps 3, 2, 1: X_s = E(Z_{s-1}), Z_{s-1} = floor(U0 + c R_{s-1})
       const double c[3] = {0.5 * dt, 0.5 * dt, dt};
       for (int sub = 3; sub >= 1; --sub) {
-        if (int rc = rhs_vjp(a, sub, a->X[sub - 1], a->Rb[sub], a->Xb)) return rc;
+        if (int rc = rhs_vjp(a, sub, a->X[sub - 1], a->Rb[sub], a->Xb, dst(t, sub))) return rc;
         k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(Z[sub - 1], a->Xb, nullptr, nullptr, a->U0b, a->Rb[sub - 1],
                                                  c[sub - 1], n, fs, a->chitiny);
         AMSS_CK(cudaGetLastError());
       }
-      if (int rc = rhs_vjp(a, 0, a->U0, a->Rb[0], a->Xb)) return rc;
+      if (int rc = rhs_vjp(a, 0, a->U0, a->Rb[0], a->Xb, dst(t, 0))) return rc;
       // the enforce pass at the start of the step: Ub = E'(U0raw)^T (U0b + Xb)
       k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(U0raw, a->U0b, a->Xb, a->Ub, nullptr, nullptr, 0.0, n, fs,
                                                a->chitiny);

@@ -81,7 +81,7 @@ struct VjpIn {
 };
 
 // Writes of the generated VJP: the centre adjoints (each written once, at the
-// point) and the D-slot adjoints (stored, then gathered by k_stencil_gather).
+// point) and the D-slot adjoints (stored, then gathered by k_stencil_gather_tiled).
 struct VjpStore {
   const AdjBlock* A;
   double* Db;   // D-slot adjoints, same layout as D
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128) k_rhs_vjp(const AdjBlock* __restrict__ bl
 // lopsided branch) and, for the advection, on the sign and value of beta(q).
 // Its transpose is gathered per target point p:
 //   fb(p) = sum_s sum_o Db_s(p - o) w_s(p - o, o),
-// so every thread owns its output point and no atomics are needed.  The
+// so every output point has one owner and no atomics are needed.  The
 // offsets are the ones the forward reads: lines o e_d, |o| <= 3 (gradient,
 // diagonal Hessian, upwind advection, KO) and planes (oa e_a + ob e_b),
 // oa, ob in {-2, -1, 1, 2} (mixed Hessian).  The advection also gives the
@@ -162,135 +162,283 @@ __device__ __forceinline__ int fit_bits(int x, int hi) {
 }
 __device__ __forceinline__ int ord_of(int f) { return (f & 1) ? 2 : ((f & 2) ? 1 : 0); }
 
-struct GatherPt {
-  const AdjBlock* A;
-  const double* Db;   // slot 0 at this point: slot s at Db[s * dfs], neighbours at int offsets
-  const double* beta; // beta^x at this point (field stride fs)
-  int dfs, fs;
-  int id[3];
-  int str[3];
-  int fb[3];   // fit bits of p's own indices
-  __device__ __forceinline__ double db(int s, int off) const { return __ldg(Db + s * dfs + off); }
+// ---------------------------------------------------------------------------
+// The transpose as a kernel: one CTA per (x-y tile, field) work item of the
+// stencil pass, marching through z like k_deriv.  The in-plane slot adjoints
+// of plane m (x/y gradients and Hessians, the mixed Hessians, adv) and the
+// shift's x/y components are staged with a 3-cell halo in shared memory by
+// cp.async (double-buffered: plane m+1 lands while plane m is used; cells
+// outside the block are zero-filled and carry zero weight).  Per plane each
+// thread gathers the in-plane terms of its own point (x, y, m) and scatters
+// the z-direction terms of its source point (x, y, m) into a register window
+// of the outputs at planes m-3 .. m+3; plane m-3 is then complete.  The mixed
+// xz / yz terms split into an in-plane gather over x (y) and a z scatter: the
+// order gate of the source point q = (x - oa, y, m) is known at plane m, and
+// the 2nd-order indicator is F2(q) - F4(q), F2 / F4 the "+-1 / +-2 fit in
+// every direction" products.
+
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// In-plane arrays of a field kind: (slot offset within the field, or -1 / -2
+// for the shift's x / y component).  Roles: gx gy hxx hyy hxy hxz hyz adv bx by.
+template <int KIND>
+struct TgMap {
+  static constexpr int NA = KIND == 0 ? 10 : (KIND == 1 ? 5 : 3);
+  static constexpr int GX = 0, GY = 1, HXX = 2, HYY = 3, HXY = 4, HXZ = 5, HYZ = 6;
+  static constexpr int ADV = KIND == 0 ? 7 : (KIND == 1 ? 2 : 0);
+  static constexpr int BX = NA - 2, BY = NA - 1;
+  __device__ static int src(int a) {
+    if (a == BX) return -1;
+    if (a == BY) return -2;
+    if (KIND == 0) {
+      constexpr int k0[8] = {0, 1, 3, 6, 4, 5, 7, 9};
+      return k0[a];
+    }
+    if (KIND == 1) return a == 0 ? 0 : (a == 1 ? 1 : 3);
+    return 0;
+  }
+};
+constexpr int kTgPlane = DPLANE;                       // cells of one staged plane (>= (W+6)(H+6))
+constexpr size_t kTgSmem = 2 * 10 * kTgPlane * sizeof(double);   // two planes of the widest kind
+
+// The plane cells one thread stages: in-plane offset of each (i + j ex0), or
+// -1 outside the block (zero-filled), fixed for the whole march.
+struct TgCells {
+  int off[DPER];
+  __device__ __forceinline__ void init(int x0, int y0, int DSX, int np, int ex0, int ex1) {
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      const int i = x0 - 3 + t % DSX, j = y0 - 3 + t / DSX;
+      off[e] = (t < np && i >= 0 && i < ex0 && j >= 0 && j < ex1) ? i + j * ex0 : (t < np ? -1 : -2);
+    }
+  }
 };
 
-// Contribution to fb(p) of every slot of field F (KIND: 0 gradient + Hessian
-// + adv, 1 gradient + adv, 2 adv only); slot base `s0`.  FAST: p is at least 6
-// cells from every face, so every point its transpose reads has full gates.
-template <int KIND, bool FAST>
-__device__ __forceinline__ double gather_field(const GatherPt& g, int s0) {
-  const Coef<double>& C = g.A->C.t;
-  const BlockView& b = g.A->b;
-  const int nsl = KIND == 0 ? 10 : (KIND == 1 ? 4 : 1);
-  const int sadv = s0 + nsl - 1;
-  double acc = 0.0;
+template <int KIND>
+__device__ __forceinline__ void tg_stage(const AdjBlock& A, const double* Db, int s0, int m, const TgCells& cells,
+                                         double* buf) {
+  const long long zoff = (long long)m * A.b.ex[0] * A.b.ex[1];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
-    const int other = FAST ? 15 : (g.fb[d1] & g.fb[d2]);
-    const int hi = b.ex[d] - 1;
-    const double kod = C.ko / C.h[d], lpd = C.d12[d];
+  for (int a = 0; a < TgMap<KIND>::NA; ++a) {
+    const int sr = TgMap<KIND>::src(a);
+    const double* base =
+        (sr >= 0 ? Db + (long long)(s0 + sr) * A.dfs : A.X + (long long)(F_BETAX - 1 - sr) * A.b.fs) + zoff;
 #pragma unroll
-    for (int o = -3; o <= 3; ++o) {
-      const int x = g.id[d] - o;
-      if (!FAST && (x < 0 || x > hi)) continue;
-      const int q = -o * g.str[d];
-      const int f = FAST ? 15 : (other & fit_bits(x, hi));
-      if (KIND != 2 && o >= -2 && o <= 2) {
-        const int ord = FAST ? 2 : ord_of(f);
-        const double w4 = o == -2 ? 1.0 : o == -1 ? -8.0 : o == 1 ? 8.0 : o == 2 ? -1.0 : 0.0;
-        const double w2 = o == -1 ? -1.0 : o == 1 ? 1.0 : 0.0;
-        if (o != 0) {
-          const double wg = ord == 2 ? C.d12[d] * w4 : (ord == 1 ? C.d2[d] * w2 : 0.0);
-          acc += g.db(s0 + d, q) * wg;
-        }
-        if (KIND == 0) {
-          const double h4 = o == 0 ? -30.0 : (o == -1 || o == 1) ? 16.0 : -1.0;
-          const double h2 = o == 0 ? -2.0 : (o == -1 || o == 1) ? 1.0 : 0.0;
-          const int sh = s0 + 3 + (d == 0 ? 0 : d == 1 ? 3 : 5);   // xx, yy, zz
-          if (FAST || ord == 2) acc += g.db(sh, q) * (C.Fdd[d] * h4);
-          else if (ord == 1 && o >= -1 && o <= 1) acc += g.db(sh, q) * (C.Sdd[d] * h2);
-        }
-      }
-      const double ab = g.db(sadv, q);
-      const double wko = o == 0 ? -20.0 : (o == 1 || o == -1) ? 15.0 : (o == 2 || o == -2) ? -6.0 : 1.0;
-      double w = (f & 4) ? kod * wko : 0.0;
-      if (f & 8) {
-        const double bq = __ldg(g.beta + d * g.fs + q);
-        const int code = FAST ? (bq > 0.0 ? 0 : 2) : lop_code(bq > 0.0, x, 0, hi);
-        w += bq * lpd * lop_w(code, o);   // zero where beta vanishes
-      }
-      acc += ab * w;
+    for (int e = 0; e < DPER; ++e) {
+      const int o = cells.off[e];
+      if (o >= -1) cp_async8(buf + a * kTgPlane + threadIdx.x + e * DTHREADS, o >= 0 ? base + o : base, o >= 0);
     }
   }
-  if (KIND == 0) {
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {   // xy, xz, yz
-      const int a = m == 2 ? 1 : 0, c = m == 0 ? 1 : 2, e = 3 - a - c;
-      const int sm = s0 + 3 + (m == 0 ? 1 : m == 1 ? 2 : 4);
-      const double F4 = m == 0 ? C.Fxy : m == 1 ? C.Fxz : C.Fyz;
-      const double S2 = m == 0 ? C.Sxy : m == 1 ? C.Sxz : C.Syz;
-      const int ha = b.ex[a] - 1, hc = b.ex[c] - 1;
-#pragma unroll
-      for (int oa = -2; oa <= 2; ++oa) {
-        if (oa == 0) continue;
-        const int xa = g.id[a] - oa;
-        if (!FAST && (xa < 0 || xa > ha)) continue;
-        const int fa = FAST ? 15 : (fit_bits(xa, ha) & g.fb[e]);
-        const double wa = oa == -2 ? 1.0 : oa == -1 ? -8.0 : oa == 1 ? 8.0 : -1.0;
-        double row = 0.0;   // FAST: the 4th-order taps of this oa summed over oc first
-#pragma unroll
-        for (int oc = -2; oc <= 2; ++oc) {
-          if (oc == 0) continue;
-          const int xc = g.id[c] - oc;
-          if (!FAST && (xc < 0 || xc > hc)) continue;
-          const double wc = oc == -2 ? 1.0 : oc == -1 ? -8.0 : oc == 1 ? 8.0 : -1.0;
-          const double v = g.db(sm, -oa * g.str[a] - oc * g.str[c]);
-          if (FAST) {
-            row += wc * v;
-          } else {
-            const int ord = ord_of(fa & fit_bits(xc, hc));
-            if (ord == 2) acc += v * (F4 * wa * wc);
-            else if (ord == 1 && oa * oa == 1 && oc * oc == 1) acc += v * (S2 * (double)(oa * oc));
-          }
-        }
-        if (FAST) acc += row * (F4 * wa);
-      }
-    }
-  }
-  return acc;
 }
 
-// Xb_F += transpose(stencil pass)(Db) of field F = blockIdx.y at every point
-// (BSSN layout, 135 slots); one thread per (point, field).  Offsets are 32-bit
-// (amss_adjoint_create bounds D_SLOTS x the field stride).
-__global__ void __launch_bounds__(128) k_stencil_gather(const AdjBlock* __restrict__ A, const double* __restrict__ Db) {
-  const BlockView& b = A->b;
-  const int F = blockIdx.y;
-  const int s0 = doff(F), n = dslots(F);
-  const int npts = (int)A->npts;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += gridDim.x * blockDim.x) {
-    GatherPt g;
-    g.A = A;
-    g.Db = Db + p;
-    g.beta = A->X + F_BETAX * b.fs + p;
-    g.dfs = (int)A->dfs;
-    g.fs = (int)b.fs;
-    g.id[0] = p % b.ex[0];
-    g.id[1] = (p / b.ex[0]) % b.ex[1];
-    g.id[2] = p / (b.ex[0] * b.ex[1]);
-    g.str[0] = 1;
-    g.str[1] = b.ex[0];
-    g.str[2] = b.ex[0] * b.ex[1];
-    bool fast = true;
-    for (int d = 0; d < 3; ++d) {
-      g.fb[d] = fit_bits(g.id[d], b.ex[d] - 1);
-      fast = fast && g.id[d] >= 6 && g.id[d] <= b.ex[d] - 7;
+// Fit bits (fit_bits) and upwind branch codes (lop_code, b > 0 in bits 0-1,
+// b < 0 in bits 2-3) of the points at index x - o, o = -3 .. 3, of one line,
+// packed 4 bits per offset; 0 bits (no gate) outside the block.
+__device__ __forceinline__ void tg_pack(int x, int hi, unsigned& fits, unsigned& codes) {
+  fits = 0u;
+  codes = 0u;
+#pragma unroll
+  for (int o = -3; o <= 3; ++o) {
+    const int xq = x - o;
+    const bool in = xq >= 0 && xq <= hi;
+    const unsigned f = in ? (unsigned)fit_bits(xq, hi) : 0u;
+    const unsigned c = in ? (unsigned)(lop_code(true, xq, 0, hi) | (lop_code(false, xq, 0, hi) << 2)) : 15u;
+    fits |= f << (4 * (o + 3));
+    codes |= c << (4 * (o + 3));
+  }
+}
+__device__ __forceinline__ int tg_bits(unsigned pk, int o) { return (int)((pk >> (4 * (o + 3))) & 15u); }
+
+template <int KIND>
+__device__ __forceinline__ void tg_column(const AdjBlock& A, const double* __restrict__ Db, int F, int x0, int y0,
+                                          double* smem) {
+  using M = TgMap<KIND>;
+  const BlockView& b = A.b;
+  const Coef<double>& C = A.C.t;
+  const int ex0 = b.ex[0], ex1 = b.ex[1], ex2 = b.ex[2];
+  const int hix = ex0 - 1, hiy = ex1 - 1, hiz = ex2 - 1;
+  const int W = deriv_tile_w(ex0), H = DTHREADS / W;
+  const int DSX = W + 6, np = DSX * (H + 6);
+  const int li = threadIdx.x % W, lj = threadIdx.x / W;
+  const int x = x0 + li, y = y0 + lj;
+  const bool mine = lj < H && x < ex0 && y < ex1;
+  const int own = (lj < H ? lj + 3 : 3) * DSX + (li + 3);
+  const int s0 = doff(F);
+  const int fbx = fit_bits(x, hix), fby = fit_bits(y, hiy);
+  unsigned pfx, pcx, pfy, pcy;
+  tg_pack(x, hix, pfx, pcx);
+  tg_pack(y, hiy, pfy, pcy);
+  const long long sz = (long long)ex0 * ex1;
+  const long long pxy = mine ? x + (long long)y * ex0 : 0;
+  const double* gzc = Db + (long long)(s0 + 2) * A.dfs + pxy;
+  const double* hzc = Db + (long long)(s0 + 8) * A.dfs + pxy;
+  const double* bzc = A.X + (long long)F_BETAZ * b.fs + pxy;
+  double* out = A.Xb + (long long)F * b.fs + pxy;
+  double acc[7];
+#pragma unroll
+  for (int t = 0; t < 7; ++t) acc[t] = 0.0;
+  const double w4[5] = {1.0, -8.0, 0.0, 8.0, -1.0};   // offsets -2..2
+
+  TgCells cells;
+  cells.init(x0, y0, DSX, np, ex0, ex1);
+  tg_stage<KIND>(A, Db, s0, 0, cells, smem);
+  cp_async_commit();
+#pragma unroll 1
+  for (int m = 0; m < ex2 + 3; ++m) {
+    if (m < ex2) {
+      if (m + 1 < ex2) tg_stage<KIND>(A, Db, s0, m + 1, cells, smem + ((m + 1) & 1) * 10 * kTgPlane);
+      cp_async_commit();
+      double gz = 0.0, hzz = 0.0, bz = 0.0;
+      if (mine) {
+        if (KIND != 2) gz = __ldg(gzc + m * sz);
+        if (KIND == 0) hzz = __ldg(hzc + m * sz);
+        bz = __ldg(bzc + m * sz);
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      const double* P = smem + (m & 1) * 10 * kTgPlane;
+      if (mine) {
+        const int fbz = fit_bits(m, hiz);
+        double ip = 0.0;
+        // x and y lines through (x, y, m); cells outside the block are zero in P
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const unsigned pf = d == 0 ? pfx : pfy, pc = d == 0 ? pcx : pcy;
+          const int st = d == 0 ? 1 : DSX;
+          const int other = (d == 0 ? fby : fbx) & fbz;
+          const double kod = C.ko / C.h[d], lpd = C.d12[d];
+#pragma unroll
+          for (int o = -3; o <= 3; ++o) {
+            const int f = other & tg_bits(pf, o);
+            const int c = own - o * st;
+            if (KIND != 2 && o >= -2 && o <= 2) {
+              const int ord = ord_of(f);
+              if (o != 0) {
+                const double wg = ord == 2 ? C.d12[d] * w4[o + 2] : (ord == 1 && (o == 1 || o == -1) ? C.d2[d] * o : 0.0);
+                ip += P[(d == 0 ? M::GX : M::GY) * kTgPlane + c] * wg;
+              }
+              if (KIND == 0) {
+                const double h4 = o == 0 ? -30.0 : (o == -1 || o == 1) ? 16.0 : -1.0;
+                const double wh = ord == 2 ? C.Fdd[d] * h4
+                                           : (ord == 1 && o >= -1 && o <= 1 ? C.Sdd[d] * (o == 0 ? -2.0 : 1.0) : 0.0);
+                ip += P[(d == 0 ? M::HXX : M::HYY) * kTgPlane + c] * wh;
+              }
+            }
+            const double ab = P[M::ADV * kTgPlane + c];
+            const double wko = o == 0 ? -20.0 : (o == 1 || o == -1) ? 15.0 : (o == 2 || o == -2) ? -6.0 : 1.0;
+            double w = (f & 4) ? kod * wko : 0.0;
+            if (f & 8) {
+              const double bq = P[(d == 0 ? M::BX : M::BY) * kTgPlane + c];
+              const int cq = tg_bits(pc, o);
+              w += bq * lpd * lop_w(bq > 0.0 ? (cq & 3) : (cq >> 2), o);
+            }
+            ip += ab * w;
+          }
+        }
+        if (KIND == 0) {
+          // xy cross stencil, gathered in the plane
+#pragma unroll
+          for (int oa = -2; oa <= 2; ++oa) {
+            if (oa == 0) continue;
+            const int fa = tg_bits(pfx, oa) & fbz;
+#pragma unroll
+            for (int ob = -2; ob <= 2; ++ob) {
+              if (ob == 0) continue;
+              const int ord = ord_of(fa & tg_bits(pfy, ob));
+              const double w = ord == 2 ? C.Fxy * w4[oa + 2] * w4[ob + 2]
+                                        : (ord == 1 && oa * oa == 1 && ob * ob == 1 ? C.Sxy * (double)(oa * ob) : 0.0);
+              ip += P[M::HXY * kTgPlane + own - oa - ob * DSX] * w;
+            }
+          }
+        }
+        acc[3] += ip;
+        // z-direction terms of the source point (x, y, m), scattered to planes m-3 .. m+3
+        const int fq = fbx & fby & fbz;
+        const int ordq = ord_of(fq);
+        if (KIND != 2) {
+#pragma unroll
+          for (int o = -2; o <= 2; ++o) {
+            if (o == 0) continue;
+            acc[3 + o] += gz * (ordq == 2 ? C.d12[2] * w4[o + 2] : (ordq == 1 && (o == 1 || o == -1) ? C.d2[2] * o : 0.0));
+          }
+        }
+        if (KIND == 0) {
+#pragma unroll
+          for (int o = -2; o <= 2; ++o) {
+            const double h4 = o == 0 ? -30.0 : (o == -1 || o == 1) ? 16.0 : -1.0;
+            acc[3 + o] += hzz * (ordq == 2 ? C.Fdd[2] * h4
+                                           : (ordq == 1 && o >= -1 && o <= 1 ? C.Sdd[2] * (o == 0 ? -2.0 : 1.0) : 0.0));
+          }
+          // xz and yz: in-plane gather along x (y) of the source points q = (x - oa, y, m), then z scatter
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const unsigned pf = e == 0 ? pfx : pfy;
+            const int st = e == 0 ? 1 : DSX;
+            const int other = (e == 0 ? fby : fbx) & fbz;
+            const int arr = e == 0 ? M::HXZ : M::HYZ;
+            double g4 = 0.0, g1 = 0.0;
+#pragma unroll
+            for (int oa = -2; oa <= 2; ++oa) {
+              if (oa == 0) continue;
+              const int f = other & tg_bits(pf, oa);
+              const double v = P[arr * kTgPlane + own - oa * st];
+              if (f & 1) g4 += w4[oa + 2] * v;
+              if ((oa == 1 || oa == -1) && (f & 2) && !(f & 1)) g1 += (double)oa * v;
+            }
+            const double F4 = e == 0 ? C.Fxz : C.Fyz, S2 = e == 0 ? C.Sxz : C.Syz;
+#pragma unroll
+            for (int oc = -2; oc <= 2; ++oc) {
+              if (oc == 0) continue;
+              double w = F4 * w4[oc + 2] * g4;
+              if (oc == 1 || oc == -1) w += S2 * (double)oc * g1;
+              acc[3 + oc] += w;
+            }
+          }
+        }
+        // adv along z: KO and the upwind stencil of the source point
+        {
+          const double ab = P[M::ADV * kTgPlane + own];
+          const int code = (fq & 8) && bz != 0.0 ? lop_code(bz > 0.0, m, 0, hiz) : 3;
+          const double kod = (fq & 4) ? C.ko / C.h[2] : 0.0;
+          const double lz = bz * C.d12[2];
+#pragma unroll
+          for (int o = -3; o <= 3; ++o) {
+            const double wko = o == 0 ? -20.0 : (o == 1 || o == -1) ? 15.0 : (o == 2 || o == -2) ? -6.0 : 1.0;
+            acc[3 + o] += ab * (kod * wko + lz * lop_w(code, o));
+          }
+        }
+      }
+      __syncthreads();   // every thread is done with plane m's buffer before plane m+2 is staged into it
     }
-    double acc;
-    if (n == 10) acc = fast ? gather_field<0, true>(g, s0) : gather_field<0, false>(g, s0);
-    else if (n == 4) acc = fast ? gather_field<1, true>(g, s0) : gather_field<1, false>(g, s0);
-    else acc = fast ? gather_field<2, true>(g, s0) : gather_field<2, false>(g, s0);
-    A->Xb[F * b.fs + p] += acc;
+    const int k = m - 3;
+    if (k >= 0 && mine) out[k * sz] += acc[0];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) acc[t] = acc[t + 1];
+    acc[6] = 0.0;
+  }
+  cp_async_wait<0>();
+}
+
+// Xb += transpose(stencil pass)(Db), one CTA per (tile, field) item of the
+// stencil pass's work list (BSSN layout, no symmetry planes).
+__global__ void __launch_bounds__(DTHREADS, 2) k_stencil_gather_tiled(const AdjBlock* __restrict__ A,
+                                                                      const DerivItem* __restrict__ items,
+                                                                      const double* __restrict__ Db) {
+  extern __shared__ __align__(16) unsigned char tg_smem[];
+  const DerivItem it = items[blockIdx.x];
+  double* smem = reinterpret_cast<double*>(tg_smem);
+  switch (dkind(it.field)) {
+    case 0: tg_column<0>(*A, Db, it.field, it.x0, it.y0, smem); break;
+    case 1: tg_column<1>(*A, Db, it.field, it.x0, it.y0, smem); break;
+    default: tg_column<2>(*A, Db, it.field, it.x0, it.y0, smem); break;
   }
 }
 
@@ -405,7 +553,7 @@ __global__ void __launch_bounds__(128) k_ham_loss(const AdjBlock* __restrict__ b
 }
 
 // Pointwise VJP of sum H^2 dV (Hb = 2 H dV on the interior cells): centre
-// adjoints into Xb, D-slot adjoints into Db (gathered by k_stencil_gather).
+// adjoints into Xb, D-slot adjoints into Db (gathered by k_stencil_gather_tiled).
 __global__ void __launch_bounds__(128) k_ham_vjp(const AdjBlock* __restrict__ blocks, int gw, double dV,
                                                  const double* H, double* Db) {
   const AdjBlock& A = blocks[blockIdx.y];
