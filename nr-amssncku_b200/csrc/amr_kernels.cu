@@ -19,7 +19,7 @@ cudaError_t launch_amr_sync(const AmrBlock* blocks, const AmrBox* boxes, const i
 cudaError_t launch_amr_prolong(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
                                int from_temp, unsigned* status, cudaStream_t s) {
   if (ntiles == 0) return cudaSuccess;
-  k_amr_prolong<<<amr_grid(ntiles), 128, 0, s>>>(blocks, boxes, tiles, ntiles, from_temp, 0, status);
+  k_amr_prolong<<<amr_grid(ntiles), 128, 0, s>>>(blocks, boxes, tiles, ntiles, from_temp, status);
   return cudaGetLastError();
 }
 

@@ -24,6 +24,13 @@ struct AmrBox {
   int n[3];
 };
 
+// Fine cells per thread of the prolongation (a run along x from an even
+// index), and the runs that cover x cells [lo0, lo0 + n0) of a box.
+constexpr int kProlongRun = 8;
+__host__ __device__ inline int prolong_runs_x(int lo0, int n0) {
+  return ((lo0 + n0) - (lo0 & ~1) + kProlongRun - 1) / kProlongRun;
+}
+
 enum AmrBuf : int { BUF_STATE = 0, BUF_STAGE_A = 1, BUF_STAGE_B = 2, BUF_TEMP = 3 };
 
 }  // namespace amss

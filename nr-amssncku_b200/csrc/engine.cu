@@ -414,10 +414,13 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   return 0;
 }
 
-static int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D) {
+// Tiles of 128 work units per box: box cells, or (prolong_nf fields) the
+// (field, run of kProlongRun fine cells along x) units the prolongation counts.
+static int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf = 0) {
   std::vector<int2> tiles;
   for (size_t m = 0; m < boxes.size(); ++m) {
-    const long long n = (long long)boxes[m].n[0] * boxes[m].n[1] * boxes[m].n[2];
+    const long long nx = prolong_nf ? prolong_runs_x(boxes[m].lo[0], boxes[m].n[0]) : boxes[m].n[0];
+    const long long n = nx * boxes[m].n[1] * boxes[m].n[2] * (prolong_nf ? prolong_nf : 1);
     for (long long p = 0; p < n; p += 128) tiles.push_back(make_int2((int)m, (int)p));
   }
   D.ntiles = (int)tiles.size();
@@ -570,7 +573,7 @@ extern "C" int amss_engine_commit(amss_engine* e) {
     if (kv.first > 0) {
       ELevel& C = e->levels[kv.first - 1];
       if (int r3 = upload_boxes(restrict_boxes(e, L, C), L.restrict_)) return r3;
-      if (int r4 = upload_boxes(prolong_boxes(e, L, C), L.prolong)) return r4;
+      if (int r4 = upload_boxes(prolong_boxes(e, L, C), L.prolong, e->nf)) return r4;
     }
   }
   if (e->prm.kernel == 0) {
