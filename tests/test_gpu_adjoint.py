@@ -206,3 +206,35 @@ def test_autograd_mass_position_gxx_against_finite_differences():
             fd = float(up - dn) / (2 * eps)
             assert abs(fd - an) <= 1e-6 * max(abs(fd), abs(an)), (trial, fd, an)
     adj.close()
+
+
+def test_gradient_matches_finite_differences_of_the_oracle_forward():
+    """The gradient against central differences (h = 1e-6) of the plain FP64
+    forward of the oracle (its level-0 step, bssn_class.C:2981-3700 restated,
+    and its constraint output), not of the GPU forward: 14^3 interior, 3 steps,
+    checkpoint every 2, two seeded directions."""
+    X, st0, bbox, h = _block(n=14, lo=-1.75, hi=1.75, noise=1e-6)
+    dt, nsteps, ck = 0.25 * h, 3, 2
+
+    def oracle_loss(st):
+        st = st.copy()
+        for _ in range(nsteps):
+            O.bssn_step_single(X, X, X, bbox, st, dt, eps=0.1)
+        return _loss_oracle(X, st, bbox)
+
+    adj = amss_b200.adjoint.Adjoint((len(X),) * 3, bbox)
+    adj.set_state(st0)
+    loss = adj.forward(dt, nsteps, ck)
+    g = adj.backward()
+    adj.close()
+    assert abs(loss - oracle_loss(st0)) <= 1e-10 * loss
+    rng = np.random.default_rng(21)
+    for trial in range(2):
+        v = rng.standard_normal(st0.shape)
+        v[18:21] = 0.0
+        v *= np.abs(st0).max(axis=(1, 2, 3), keepdims=True).clip(1e-3, 1.0)
+        v[0] = rng.standard_normal(st0.shape[1:]) * (1.0 + st0[0])
+        v[17] = rng.standard_normal(st0.shape[1:]) * (1.0 + st0[17])
+        an = float(np.sum(g * v))
+        fd = (oracle_loss(st0 + 1e-6 * v) - oracle_loss(st0 - 1e-6 * v)) / 2e-6
+        assert abs(fd - an) <= 1e-6 * max(abs(fd), abs(an)), (trial, fd, an)
