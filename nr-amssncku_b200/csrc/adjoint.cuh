@@ -101,10 +101,27 @@ __device__ __forceinline__ bool on_face_point(const BlockView& b, int i, int j, 
 // are written (zero where the right-hand side does not read the value, and
 // everywhere at face points, whose right-hand side is the Sommerfeld rule), so
 // neither needs clearing first.
+// L2 prefetch (warp 0) of the rows [p0, p0 + 128) of nrows arrays at stride
+// `stride` from base: the tile's points only, rounded up to 16 bytes, which
+// stays inside rows padded to a multiple of 64 values.
+__device__ __forceinline__ void prefetch_tile_rows(const double* base, long long stride, int nrows, long long p0,
+                                                   long long npts) {
+  if (threadIdx.x >= 32 || p0 >= npts) return;
+  const long long nel = npts - p0 < 128 ? npts - p0 : 128;
+  const unsigned bytes = (unsigned)((nel * 8 + 15) / 16 * 16);
+  for (int r = threadIdx.x; r < nrows; r += 32)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + r * stride + p0), "r"(bytes) : "memory");
+}
+
 __global__ void __launch_bounds__(128) k_rhs_vjp(const AdjBlock* __restrict__ blocks, double* Db) {
   const AdjBlock& A = blocks[blockIdx.y];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < A.npts;
        p += (long long)gridDim.x * blockDim.x) {
+    // this tile's rows meet the point function's one-by-one loads in L2
+    const long long p0 = p - threadIdx.x;
+    prefetch_tile_rows(A.D, A.dfs, D_SLOTS, p0, A.npts);
+    prefetch_tile_rows(A.X, A.b.fs, NFIELDS_BSSN, p0, A.npts);
+    prefetch_tile_rows(A.Rb, A.b.fs, NFIELDS_BSSN, p0, A.npts);
     int i, j, k;
     point_ijk(p, A.b.ex, i, j, k);
     if (on_face_point(A.b, i, j, k)) {
@@ -257,6 +274,34 @@ __device__ __forceinline__ void tg_pack(int x, int hi, unsigned& fits, unsigned&
 }
 __device__ __forceinline__ int tg_bits(unsigned pk, int o) { return (int)((pk >> (4 * (o + 3))) & 15u); }
 
+// L2 prefetch, one 128-byte line per thread and step, of plane m's tile rows
+// (with halo) of every array the march reads, a few planes before it is staged.
+template <int KIND>
+__device__ __forceinline__ void tg_prefetch(const AdjBlock& A, const double* Db, int s0, int m, int x0, int y0,
+                                            int W, int H) {
+  const BlockView& b = A.b;
+  const int ex0 = b.ex[0], ex1 = b.ex[1];
+  const int xl = x0 - 3 < 0 ? 0 : x0 - 3, xh = x0 + W + 3 > ex0 ? ex0 : x0 + W + 3;
+  const int yl = y0 - 3 < 0 ? 0 : y0 - 3, yh = y0 + H + 3 > ex1 ? ex1 : y0 + H + 3;
+  const int lpr = ((xh - xl) * 8 + 127) / 128, nr = yh - yl;
+  const int na = TgMap<KIND>::NA + (KIND == 0 ? 3 : (KIND == 1 ? 2 : 1));   // + the z-column arrays
+  const long long zoff = (long long)m * ex0 * ex1 + xl;
+  for (int t = threadIdx.x; t < na * nr * lpr; t += DTHREADS) {
+    const int a = t / (nr * lpr), rem = t - a * nr * lpr, r = rem / lpr, c = rem - r * lpr;
+    const double* base;
+    if (a < TgMap<KIND>::NA) {
+      const int sr = TgMap<KIND>::src(a);
+      base = sr >= 0 ? Db + (long long)(s0 + sr) * A.dfs : A.X + (long long)(F_BETAX - 1 - sr) * b.fs;
+    } else {
+      const int z = a - TgMap<KIND>::NA;   // beta^z, then gz and hzz as the kind has them
+      base = z == 0 ? A.X + (long long)F_BETAZ * b.fs : Db + (long long)(s0 + (z == 1 ? 2 : 8)) * A.dfs;
+    }
+    const char* row = (const char*)(base + zoff + (long long)(yl + r) * ex0);
+    const int off = c * 128 < (xh - xl - 1) * 8 ? c * 128 : (xh - xl - 1) * 8;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(row + off));
+  }
+}
+
 template <int KIND>
 __device__ __forceinline__ void tg_column(const AdjBlock& A, const double* __restrict__ Db, int F, int x0, int y0,
                                           double* smem) {
@@ -296,6 +341,7 @@ __device__ __forceinline__ void tg_column(const AdjBlock& A, const double* __res
     if (m < ex2) {
       if (m + 1 < ex2) tg_stage<KIND>(A, Db, s0, m + 1, cells, smem + ((m + 1) & 1) * 10 * kTgPlane);
       cp_async_commit();
+      if (m + 5 < ex2) tg_prefetch<KIND>(A, Db, s0, m + 5, x0, y0, W, H);
       double gz = 0.0, hzz = 0.0, bz = 0.0;
       if (mine) {
         if (KIND != 2) gz = __ldg(gzc + m * sz);

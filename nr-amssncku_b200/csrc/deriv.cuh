@@ -31,6 +31,9 @@ namespace amss {
 // (deriv_tile) so that narrow blocks do not leave lanes idle: W = the block's
 // x extent split into pieces of at most 64, H = DTHREADS / W rows.
 constexpr int DTHREADS = 256;
+#ifndef AMSS_DERIV_PREFETCH   // planes beyond the register fetch whose tile rows are prefetched into L2 (0: none)
+#define AMSS_DERIV_PREFETCH 4
+#endif
 constexpr int DWMAX = 64;
 constexpr int DPLANE = 704;                 // >= (W + 6) (H + 6) for every admissible W
 constexpr int DRING = 5;                    // resident planes: k-1 (being replaced), k .. k+3
@@ -218,6 +221,25 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
 #pragma unroll 1
   for (int k = 0; k < ex2; ++k) {
     P.fetch(k + 4);   // in flight while plane k is computed
+#if AMSS_DERIV_PREFETCH
+    {
+      // warp 0 asks L2 for the tile rows (with halo) of plane k+4+AMSS_DERIV_PREFETCH,
+      // one 128-byte line per lane, so the register fetch of that plane meets L2
+      const int kk = k + 4 + AMSS_DERIV_PREFETCH;
+      if (threadIdx.x < 32 && kk < ex2) {
+        const int xl = x0 - 3 < 0 ? 0 : x0 - 3, xh = x0 + W + 3 > ex0 ? ex0 : x0 + W + 3;
+        const int yl = y0 - 3 < 0 ? 0 : y0 - 3, yh = y0 + H + 3 > ex1 ? ex1 : y0 + H + 3;
+        const int lpr = (int)(((xh - xl) * sizeof(S) + 127) / 128);   // lines per row
+        for (int t = threadIdx.x; t < lpr * (yh - yl); t += 32) {
+          const int r = t / lpr, c = t - r * lpr;
+          const char* row = (const char*)(src + xl + (long long)(yl + r) * ex0 + (long long)kk * ex0 * ex1);
+          const long long off = (long long)c * 128 < (long long)((xh - xl - 1) * sizeof(S)) ? (long long)c * 128
+                                                                                           : (long long)((xh - xl - 1) * sizeof(S));
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + off));
+        }
+      }
+    }
+#endif
     const A* qk = ring + ring_slot(k) * DPLANE + own;
     c[6] = ring[ring_slot(k + 3) * DPLANE + own];
     if constexpr (KIND == 0) {

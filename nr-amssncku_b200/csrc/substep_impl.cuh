@@ -10,8 +10,8 @@
 #ifndef AMSS_SUBSTEP_MINB_F32   // the same for FP32 arithmetic (fits 168 registers without spills)
 #define AMSS_SUBSTEP_MINB_F32 3
 #endif
-#ifndef AMSS_POINTWISE_PREFETCH   // L2 prefetch of the next tile's rows in the register pass
-#define AMSS_POINTWISE_PREFETCH 0
+#ifndef AMSS_POINTWISE_PREFETCH   // L2 prefetch in the register pass: 0 none, 1 the next tile's rows, 2 this
+#define AMSS_POINTWISE_PREFETCH 2     // tile's, 3 both
 #endif
 
 namespace amss {
@@ -30,26 +30,37 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
     const int2 tile = tiles[t];
     const StepBlock<T>& B = blocks[tile.x];
 #if AMSS_POINTWISE_PREFETCH
-    // split form: pull the rows of this CTA's next tile (D slots, stage
-    // input, u0, K) into L2 while this tile computes, so its loads meet L2
-    // rather than HBM latency
+    // split form: pull the rows of a tile (D slots, stage input, u0, K) into
+    // L2 -- the next tile's while this one computes, or this tile's before its
+    // point function issues its loads one by one -- so they meet L2 rather
+    // than HBM latency
     if constexpr (SPLIT) {
-      if (threadIdx.x < 32 && t + (int)gridDim.x < ntiles) {
-        const int2 nt = tiles[t + gridDim.x];
+#pragma unroll 1
+     for (int pass = 0; pass < 2; ++pass) {
+      const int mode = AMSS_POINTWISE_PREFETCH;
+      if (pass == 0 ? !(mode & 2) : !(mode & 1)) continue;
+      const int tn = pass == 0 ? t : t + (int)gridDim.x;
+      if (threadIdx.x < 32 && tn < ntiles) {
+        const int2 nt = tiles[tn];
         const StepBlock<T>& N = blocks[nt.x];
         const long long fs = N.b.fs, q0 = nt.y;
         const int cur = N.lvl[0];
         const SI* nin = sub == 0 ? (const SI*)N.tl[cur] : (const SI*)N.stage[sub == 2 ? 1 : 0];
+        // the tile's points only (the last tile of a block is short), rounded up to
+        // 16 bytes: still inside the block's field, whose stride is a multiple of 64
+        const long long nel = N.npts - q0 < 128 ? N.npts - q0 : 128;
+        auto len = [&](int es) { return (unsigned)((nel * es + 15) / 16 * 16); };
         for (int r = threadIdx.x; r < D_SLOTS + 72; r += 32) {
           const void* a;
           unsigned bytes;
-          if (r < D_SLOTS) { a = D + N.doff + r * dfs + q0; bytes = 128 * sizeof(T); }
-          else if (r < D_SLOTS + 24) { a = nin + (r - D_SLOTS) * fs + q0; bytes = 128 * sizeof(SI); }
-          else if (r < D_SLOTS + 48) { a = N.tl[cur] + (r - D_SLOTS - 24) * fs + q0; bytes = 128 * sizeof(double); }
-          else { a = N.K + (r - D_SLOTS - 48) * fs + q0; bytes = 128 * sizeof(double); }
+          if (r < D_SLOTS) { a = D + N.doff + r * dfs + q0; bytes = len(sizeof(T)); }
+          else if (r < D_SLOTS + 24) { a = nin + (r - D_SLOTS) * fs + q0; bytes = len(sizeof(SI)); }
+          else if (r < D_SLOTS + 48) { a = N.tl[cur] + (r - D_SLOTS - 24) * fs + q0; bytes = len(sizeof(double)); }
+          else { a = N.K + (r - D_SLOTS - 48) * fs + q0; bytes = len(sizeof(double)); }
           asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
         }
       }
+     }
     }
 #endif
     const long long p = (long long)tile.y + threadIdx.x;
