@@ -281,7 +281,9 @@ long long amss_engine_launch_count(amss_engine* e);
  * from every face of H^2 dx dy dz, H the Hamiltonian constraint of the final
  * state.  The gradient is dL/d(initial state) (24 fields, field-major, the
  * same host layout as amss_engine_set_state), computed by reverse-mode over
- * RK4 with a checkpoint every `ck` steps (each segment recomputed once). */
+ * RK4 with a checkpoint every `ck` steps: every segment but the last is recomputed
+ * once; the forward keeps the last segment's stages, and, where the device has room,
+ * every substep's stencil terms of a segment (4 ck x 135 fields). */
 typedef struct amss_adjoint amss_adjoint;
 
 /* chitiny: the lowerboundset floor on chi (bssn_class.C:179, :3156).  NULL on failure. */

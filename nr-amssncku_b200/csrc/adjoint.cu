@@ -95,6 +95,7 @@ struct amss_adjoint {
   int seg_cap = 0;
   double* Dseg = nullptr;                // the segment's stencil terms, per step and substep (if HBM allows)
   int dseg_cap = 0;
+  bool last_seg_ready = false;           // the forward left the last segment's states (and terms) in seg / Dseg
   double* Ub = nullptr;
   double* U0b = nullptr;
   double* Rb[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -367,6 +368,35 @@ static int loss_and_grad(amss_adjoint* a, double* loss, bool want_grad) {
   return 0;
 }
 
+// Segment storage: per step U0raw, Z0, Z1, Z2, then the segment's last U_new;
+// and, when the device has room for them, the stencil terms of every substep
+// of a segment (4 ck arrays of D_SLOTS fields; 92 GB at 96^3 + ghosts with
+// ck = 20), so the reverse sweep reads them instead of recomputing them.
+static int reserve_segment(amss_adjoint* a) {
+  const size_t sb = state_bytes(a);
+  const int need = 4 * a->ck + 1;
+  if (a->seg_cap < need) {
+    if (a->seg) cudaFree(a->seg);
+    a->seg = nullptr;
+    AMSS_CK(cudaMalloc(&a->seg, (size_t)need * sb));
+    a->seg_cap = need;
+  }
+  const size_t dsz = (size_t)D_SLOTS * a->fs;
+  if (a->dseg_cap < 4 * a->ck) {
+    if (a->Dseg) cudaFree(a->Dseg);
+    a->Dseg = nullptr;
+    a->dseg_cap = 0;
+    size_t free_b = 0, total_b = 0;
+    const size_t want = (size_t)4 * a->ck * dsz * sizeof(double);
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b > want + ((size_t)4 << 30) &&
+        cudaMalloc(&a->Dseg, want) == cudaSuccess)
+      a->dseg_cap = 4 * a->ck;
+    else
+      (void)cudaGetLastError();   // not enough room: the reverse sweep recomputes them
+  }
+  return 0;
+}
+
 extern "C" int amss_adjoint_forward(amss_adjoint* a, double dt, int nsteps, int ck, double* loss) {
   if (!a || !loss || nsteps < 0 || ck < 1) return amss_fail(AMSS_ERR_ARG, "amss_adjoint_forward: bad arguments");
   a->dt = dt;
@@ -379,14 +409,33 @@ extern "C" int amss_adjoint_forward(amss_adjoint* a, double dt, int nsteps, int 
     a->ckpt.assign(nck + 1, nullptr);
     for (int m = 0; m <= nck; ++m) AMSS_CK(cudaMalloc(&a->ckpt[m], sb));
   }
+  a->last_seg_ready = false;
+  if (int rc = reserve_segment(a)) return rc;
   cudaStream_t s = a->stream;
   double* Zs1 = a->Zs + (size_t)NFIELDS_BSSN * a->fs;
   double* Zs2 = a->Zs + (size_t)2 * NFIELDS_BSSN * a->fs;
+  // the steps of the last segment write their states (and stencil terms)
+  // straight into the segment storage, which the reverse sweep starts from
+  const long long m = (long long)NFIELDS_BSSN * a->fs;
+  const size_t dsz = (size_t)D_SLOTS * a->fs;
+  const int nlast = nck > 0 ? (nck - 1) * ck : 0;
   for (int n = 0; n < nsteps; ++n) {
     if (n % ck == 0) AMSS_CK(cudaMemcpyAsync(a->ckpt[n / ck], a->U, sb, cudaMemcpyDeviceToDevice, s));
-    if (int rc = fwd_step(a, a->U, a->U, a->Zs, Zs1, Zs2)) return rc;
+    if (n >= nlast) {
+      const int t = n - nlast;
+      double* st0 = a->seg + (size_t)4 * t * m;
+      AMSS_CK(cudaMemcpyAsync(st0, a->U, sb, cudaMemcpyDeviceToDevice, s));
+      double* const dts[4] = {a->Dseg + (size_t)(4 * t) * dsz, a->Dseg + (size_t)(4 * t + 1) * dsz,
+                              a->Dseg + (size_t)(4 * t + 2) * dsz, a->Dseg + (size_t)(4 * t + 3) * dsz};
+      if (int rc = fwd_step(a, a->U, a->U, st0 + m, st0 + 2 * m, st0 + 3 * m, a->Dseg ? dts : nullptr)) return rc;
+    } else {
+      if (int rc = fwd_step(a, a->U, a->U, a->Zs, Zs1, Zs2)) return rc;
+    }
   }
+  if (nsteps > 0)
+    AMSS_CK(cudaMemcpyAsync(a->seg + (size_t)4 * (nsteps - nlast) * m, a->U, sb, cudaMemcpyDeviceToDevice, s));
   AMSS_CK(cudaMemcpyAsync(a->ckpt[nck], a->U, sb, cudaMemcpyDeviceToDevice, s));
+  a->last_seg_ready = nsteps > 0;
   if (int rc = loss_and_grad(a, loss, false)) return rc;
   a->forward_done = true;
   return 0;
@@ -399,31 +448,9 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
   const size_t sb = state_bytes(a);
   const long long n = a->npts, fs = a->fs, m = (long long)NFIELDS_BSSN * fs;
   const int nck = (a->nsteps + a->ck - 1) / a->ck;
-  // per step of a segment: U0raw, Z0, Z1, Z2; then the segment's last U_new
-  const int need = 4 * a->ck + 1;
-  if (a->seg_cap < need) {
-    if (a->seg) cudaFree(a->seg);
-    a->seg = nullptr;
-    AMSS_CK(cudaMalloc(&a->seg, (size_t)need * sb));
-    a->seg_cap = need;
-  }
+  if (int rc = reserve_segment(a)) return rc;   // allocated by the forward already
   auto st = [&](int slot) { return a->seg + (size_t)slot * m; };
-  // The stencil terms of every substep of a segment (4 ck arrays of D_SLOTS
-  // fields; 92 GB at 96^3 + ghosts with ck = 20) are kept when the device has
-  // room for them, so the reverse sweep reads them instead of recomputing them.
   const size_t dsz = (size_t)D_SLOTS * fs;
-  if (a->dseg_cap < 4 * a->ck) {
-    if (a->Dseg) cudaFree(a->Dseg);
-    a->Dseg = nullptr;
-    a->dseg_cap = 0;
-    size_t free_b = 0, total_b = 0;
-    const size_t want = (size_t)4 * a->ck * dsz * sizeof(double);
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b > want + ((size_t)4 << 30) &&
-        cudaMalloc(&a->Dseg, want) == cudaSuccess)
-      a->dseg_cap = 4 * a->ck;
-    else
-      (void)cudaGetLastError();   // not enough room: recompute instead
-  }
   auto dst = [&](int t, int sub) { return a->Dseg ? a->Dseg + (size_t)(4 * t + sub) * dsz : nullptr; };
   // dL/dU at the final time
   double loss = 0;
@@ -433,14 +460,18 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
   for (int sg = nck - 1; sg >= 0; --sg) {
     const int n0 = sg * a->ck, n1 = std::min(n0 + a->ck, a->nsteps), ns = n1 - n0;
     // recompute the segment, storing what the reverse sweep linearizes about
-    AMSS_CK(cudaMemcpyAsync(a->U, a->ckpt[sg], sb, cudaMemcpyDeviceToDevice, s));
-    for (int t = 0; t < ns; ++t) {
-      AMSS_CK(cudaMemcpyAsync(st(4 * t), a->U, sb, cudaMemcpyDeviceToDevice, s));
-      double* const dts[4] = {dst(t, 0), dst(t, 1), dst(t, 2), dst(t, 3)};
-      if (int rc = fwd_step(a, a->U, a->U, st(4 * t + 1), st(4 * t + 2), st(4 * t + 3), a->Dseg ? dts : nullptr))
-        return rc;
+    // (the last one the forward left in place)
+    if (!(sg == nck - 1 && a->last_seg_ready)) {
+      AMSS_CK(cudaMemcpyAsync(a->U, a->ckpt[sg], sb, cudaMemcpyDeviceToDevice, s));
+      for (int t = 0; t < ns; ++t) {
+        AMSS_CK(cudaMemcpyAsync(st(4 * t), a->U, sb, cudaMemcpyDeviceToDevice, s));
+        double* const dts[4] = {dst(t, 0), dst(t, 1), dst(t, 2), dst(t, 3)};
+        if (int rc = fwd_step(a, a->U, a->U, st(4 * t + 1), st(4 * t + 2), st(4 * t + 3), a->Dseg ? dts : nullptr))
+          return rc;
+      }
+      AMSS_CK(cudaMemcpyAsync(st(4 * ns), a->U, sb, cudaMemcpyDeviceToDevice, s));
     }
-    AMSS_CK(cudaMemcpyAsync(st(4 * ns), a->U, sb, cudaMemcpyDeviceToDevice, s));
+    a->last_seg_ready = false;   // the segment storage now holds this segment
     for (int t = ns - 1; t >= 0; --t) {
       double* U0raw = st(4 * t);
       double* Z[3] = {st(4 * t + 1), st(4 * t + 2), st(4 * t + 3)};
@@ -458,13 +489,13 @@ extern "C" int amss_adjoint_backward(amss_adjoint* a, double* grad) {
       const double c[3] = {0.5 * dt, 0.5 * dt, dt};
       for (int sub = 3; sub >= 1; --sub) {
         if (int rc = rhs_vjp(a, sub, a->X[sub - 1], a->Rb[sub], a->Xb, dst(t, sub))) return rc;
-        k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(Z[sub - 1], a->Xb, nullptr, nullptr, a->U0b, a->Rb[sub - 1],
+        k_enforce_vjp<true><<<grid_of(n), 128, 0, s>>>(Z[sub - 1], a->Xb, nullptr, nullptr, a->U0b, a->Rb[sub - 1],
                                                  c[sub - 1], n, fs, a->chitiny);
         AMSS_CK(cudaGetLastError());
       }
       if (int rc = rhs_vjp(a, 0, a->U0, a->Rb[0], a->Xb, dst(t, 0))) return rc;
       // the enforce pass at the start of the step: Ub = E'(U0raw)^T (U0b + Xb)
-      k_enforce_vjp<<<grid_of(n), 128, 0, s>>>(U0raw, a->U0b, a->Xb, a->Ub, nullptr, nullptr, 0.0, n, fs,
+      k_enforce_vjp<false><<<grid_of(n), 128, 0, s>>>(U0raw, a->U0b, a->Xb, a->Ub, nullptr, nullptr, 0.0, n, fs,
                                                a->chitiny);
       AMSS_CK(cudaGetLastError());
       a->launches += 9;

@@ -17,6 +17,10 @@
 // (ham_vjp), the loss integrand of the adjoint driver.
 #pragma once
 #include "rhs_vjp_gen.cuh"
+
+#ifndef AMSS_ENFVJP_MINB   // resident CTAs per SM the enforce VJP is compiled for
+#define AMSS_ENFVJP_MINB 4
+#endif
 #include "substep_common.cuh"
 
 namespace amss {
@@ -641,11 +645,15 @@ struct EnfOut {
 // result: Zb = mask(Z) E'(Z)^T (E1 + E2) per point (chi masked where the floor
 // held Z at chitiny; E2 may be null), then
 //   out = Zb (if out), acc0 += Zb (if acc0), acc1 += c1 Zb (if acc1).
-__global__ void __launch_bounds__(128) k_enforce_vjp(const double* __restrict__ Z, const double* E1,
-                                                     const double* E2, double* out, double* acc0, double* acc1,
+// ACC: acc0 += Zb, acc1 += c1 Zb (a substep's reverse); else out = Zb with
+// E2 added to E1 (the step start).  No two arrays alias.
+template <bool ACC>
+__global__ void __launch_bounds__(128, AMSS_ENFVJP_MINB) k_enforce_vjp(const double* __restrict__ Z, const double* __restrict__ E1,
+                                                     const double* __restrict__ E2, double* __restrict__ out,
+                                                     double* __restrict__ acc0, double* __restrict__ acc1,
                                                      double c1, long long n, long long fs, double chitiny) {
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    EnfIn in{Z, E1, E2, fs, p};
+    EnfIn in{Z, E1, ACC ? nullptr : E2, fs, p};
     EnfOut eo;
     enforce_vjp<double>(in, eo);
     const bool floor_held = Z[F_CHI * fs + p] == chitiny;
@@ -654,11 +662,14 @@ __global__ void __launch_bounds__(128) k_enforce_vjp(const double* __restrict__ 
       const long long o = f * fs + p;
       double v;
       if (f >= F_GXX && f <= F_AZZ) v = eo.zb[f - F_GXX];
-      else v = E2 ? E1[o] + E2[o] : E1[o];
+      else v = ACC ? E1[o] : E1[o] + E2[o];
       if (f == F_CHI && floor_held) v = 0.0;
-      if (out) out[o] = v;
-      if (acc0) acc0[o] += v;
-      if (acc1) acc1[o] += c1 * v;
+      if (ACC) {
+        acc0[o] += v;
+        acc1[o] += c1 * v;
+      } else {
+        out[o] = v;
+      }
     }
   }
 }
