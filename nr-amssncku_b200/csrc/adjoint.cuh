@@ -18,6 +18,12 @@
 #pragma once
 #include "rhs_vjp_gen.cuh"
 
+#ifndef AMSS_BETA_UNROLL   // fields per unrolled step of the shift-adjoint loop
+#define AMSS_BETA_UNROLL 4
+#endif
+namespace amss {
+constexpr int kBetaUnroll = AMSS_BETA_UNROLL;
+}
 #ifndef AMSS_ENFVJP_MINB   // resident CTAs per SM the enforce VJP is compiled for
 #define AMSS_ENFVJP_MINB 4
 #endif
@@ -503,6 +509,9 @@ __global__ void __launch_bounds__(128) k_beta_adjoint(const AdjBlock* __restrict
     int id[3];
     point_ijk(p, b.ex, id[0], id[1], id[2]);
     const long long str[3] = {1, b.ex[0], (long long)b.ex[0] * b.ex[1]};
+    // face points (no advection term, zero adv adjoint) are skipped: every
+    // other point's upwind stencil lies inside the block
+    if (on_face_point(b, id[0], id[1], id[2])) continue;
     if (!(fit_bits(id[0], b.ex[0] - 1) & fit_bits(id[1], b.ex[1] - 1) & fit_bits(id[2], b.ex[2] - 1) & 8)) continue;
     int code[3];
     bool any = false;
@@ -512,21 +521,29 @@ __global__ void __launch_bounds__(128) k_beta_adjoint(const AdjBlock* __restrict
       any = any || code[d] != 3;
     }
     if (!any) continue;
+    // per direction: the five points of the upwind stencil the forward used and
+    // their weights (all zero where it added nothing), so the field loop has no
+    // branches and its loads can be issued together
+    long long o0[3], st[3];
+    double w[3][5];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int c = code[d];
+      st[d] = c == 3 ? 0 : str[d];
+      o0[d] = c == 0 ? -1 : (c == 1 ? -2 : -3);
+#pragma unroll
+      for (int t = 0; t < 5; ++t) w[d][t] = c == 3 ? 0.0 : lop_w(c, (int)o0[d] + t);
+    }
     double bb[3] = {0.0, 0.0, 0.0};
-#pragma unroll 1
+#pragma unroll kBetaUnroll
     for (int F = 0; F < NFIELDS_BSSN; ++F) {
       const double ab = Db[(doff(F) + dslots(F) - 1) * A->dfs + p];
-      if (ab == 0.0) continue;
       const double* X = A->X + F * b.fs + p;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        if (code[d] == 3) continue;
         double u = 0.0;
 #pragma unroll
-        for (int o = -3; o <= 3; ++o) {
-          const double w = lop_w(code[d], o);
-          if (w != 0.0) u += w * X[o * str[d]];
-        }
+        for (int t = 0; t < 5; ++t) u += w[d][t] * X[(o0[d] + t) * st[d]];
         bb[d] += ab * C.d12[d] * u;
       }
     }
