@@ -25,7 +25,8 @@ namespace amss {
 """
 
 
-def main():
+def generate():
+    """The text of csrc/rhs_vjp_gen.cuh from the tapes."""
     parts = [HDR]
     for name, fn in (("rhs_vjp_bssn", "tape_bssn.txt"), ("rhs_vjp_z4c", "tape_z4c.txt"),
                      ("ham_vjp", "tape_ham.txt"), ("enforce_vjp", "tape_enforce.txt")):
@@ -35,8 +36,12 @@ def main():
     parts.append(TP.emit_fwd(TP.Tape(os.path.join(HERE, "tape_ham.txt")), "ham_fwd", 99))
     parts.append("\n")
     parts.append("}  // namespace amss\n")
+    return "".join(parts)
+
+
+def main():
     with open(os.path.join(HERE, "..", "csrc", "rhs_vjp_gen.cuh"), "w") as fh:
-        fh.write("".join(parts))
+        fh.write(generate())
 
 
 if __name__ == "__main__":

@@ -128,3 +128,27 @@ def test_tape_reverse_sweep_matches_finite_differences(name):
     dn = tp.evaluate({f: c[f] - h * dc[f] for f in c}, {s: d[s] - h * dd[s] for s in d})
     rhs = sum(np.sum(rb[f] * (up[f] - dn[f]) / (2 * h)) for f in tp.outputs)
     assert abs(lhs - rhs) <= 1e-7 * abs(lhs), (lhs, rhs)
+
+
+def test_tapes_are_the_current_kernels():
+    """gen/trace_rhs.cpp, compiled from the kernels' point functions as they are
+    now, records exactly the committed tapes, and the committed generated VJP
+    header is what gen/emit.py makes of them: the adjoint differentiates the
+    forward that runs."""
+    import shutil
+    import subprocess
+    import tempfile
+    gen = os.path.join(HERE, "..", "nr-amssncku_b200", "gen")
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "trace_rhs")
+        subprocess.run([cxx, "-std=c++17", "-O0", "-o", exe, os.path.join(gen, "trace_rhs.cpp")], check=True)
+        for mode in ("bssn", "z4c", "ham", "enforce"):
+            out = subprocess.run([exe, mode], check=True, capture_output=True, text=True).stdout
+            with open(os.path.join(gen, f"tape_{mode}.txt")) as fh:
+                assert out == fh.read(), mode
+    import emit
+    with open(os.path.join(HERE, "..", "nr-amssncku_b200", "csrc", "rhs_vjp_gen.cuh")) as fh:
+        assert emit.generate() == fh.read()
