@@ -6,15 +6,16 @@
 //   1. pointwise: rhs_vjp_bssn (generated from a recording of the kernel's
 //      own point function, rhs_vjp_gen.cuh) gives the adjoints of u(p) and of
 //      every D slot;
-//   2. transpose of the stencils: each D-slot adjoint is scattered back onto
-//      the field values its stencil read, with the same order / KO / lopsided
-//      gates and the same mirroring of negative indices (parity of the field)
-//      as the forward; the upwinded advection also gives the shift its
-//      adjoint, Rb * (unweighted upwind derivative).
-// Outer-face points take the transpose of the Sommerfeld rule instead.  All
-// contributions are accumulated with atomicAdd into the adjoint of the stage
-// input.  The same machinery gives the VJP of the Hamiltonian constraint
-// (ham_vjp), the loss integrand of the adjoint driver.
+//   2. transpose of the stencils (k_stencil_gather_tiled): the D-slot
+//      adjoints of the points whose stencils read a field value are gathered
+//      onto it, with the same order / KO / lopsided gates as the forward
+//      (blocks without symmetry planes); the upwinded advection also gives
+//      the shift its adjoint, Rb * (unweighted upwind derivative)
+//      (k_beta_adjoint).
+// Outer-face points take the transpose of the Sommerfeld rule instead
+// (k_face_vjp, atomicAdd onto the few points it reaches).  The same machinery
+// gives the VJP of the Hamiltonian constraint (ham_vjp), the loss integrand of
+// the adjoint driver.
 #pragma once
 #include "rhs_vjp_gen.cuh"
 
@@ -57,8 +58,8 @@ __device__ __forceinline__ int slot_field(int s) {
   return t.f[s];
 }
 
-// Scatter target: the field value at (i, j, k), mirrored cell-centred (with the
-// field's parity) where an index is negative, as the forward's padded reads.
+// Scatter target of the Sommerfeld transpose: the field value at (i, j, k),
+// mirrored cell-centred (with the field's parity) where an index is negative.
 struct Scatter {
   const AdjBlock* A;
   __device__ __forceinline__ void add(int F, int i, int j, int k, double v) const {
@@ -68,15 +69,6 @@ struct Scatter {
     if (k < 0) { k = -k - 1; if (soa_sign(F, 2) < 0) v = -v; }
     if (i >= b.ex[0] || j >= b.ex[1] || k >= b.ex[2]) return;   // never read by a gated stencil
     atomicAdd(A->Xb + F * b.fs + i + (long long)j * b.ex[0] + (long long)k * b.ex[0] * b.ex[1], v);
-  }
-  __device__ __forceinline__ double get(int F, int i, int j, int k) const {
-    const BlockView& b = A->b;
-    bool neg = false;
-    if (i < 0) { i = -i - 1; neg ^= soa_sign(F, 0) < 0; }
-    if (j < 0) { j = -j - 1; neg ^= soa_sign(F, 1) < 0; }
-    if (k < 0) { k = -k - 1; neg ^= soa_sign(F, 2) < 0; }
-    const double v = A->X[F * b.fs + i + (long long)j * b.ex[0] + (long long)k * b.ex[0] * b.ex[1]];
-    return neg ? -v : v;
   }
 };
 
