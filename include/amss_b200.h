@@ -271,6 +271,18 @@ void* amss_engine_stream(amss_engine* e);
 /* Number of kernel launches the engine issued so far. */
 long long amss_engine_launch_count(amss_engine* e);
 
+/* The constraint monitor of one level (bssn_class.C:7463-7484,
+ * Z4c_class.C:2491-2510, with Parallel::L2Norm, Parallel.C:4214-4243, and
+ * l2normhelper, fmisc.f90:1263-1309): norms[0..6] = sqrt(sum c^2 dx dy dz) of
+ * the Hamiltonian, the 3 momentum and the 3 Gamma constraints (compute_rhs_bssn
+ * with co = 0, bssn_rhs.f90:1044-1135; constraint_bssn for Z4c) of the level's
+ * current state, norms[7] that of Theta (Z4c; 0 for BSSN), in FP64 whatever
+ * the engine's precision.  Cells: a block added by bbox contributes
+ * its array less 3 ghost cells on each side whose outer cell is not within one
+ * cell of its patch box; an AMR block its owned cells inside its patch,
+ * buffer cells included.  Waits for the engine's stream. */
+int amss_engine_constraint_norms(amss_engine* e, int level, double norms[8]);
+
 /* ---- Adjoint of a single-patch BSSN evolution (no reference counterpart:
  * the reference has no derivative code; the forward it differentiates is the
  * level-0 RK4 step of bssn_class::Step, bssn_class.C:2981-3700, with

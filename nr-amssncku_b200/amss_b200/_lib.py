@@ -58,6 +58,7 @@ def lib():
     L.amss_engine_level_points.restype = ctypes.c_longlong
     L.amss_engine_launch_count.argtypes = [ctypes.c_void_p]
     L.amss_engine_launch_count.restype = ctypes.c_longlong
+    L.amss_engine_constraint_norms.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
     L.get_lousto_nbhs_.restype = ctypes.c_int
     L.amss_lousto_vjp.restype = ctypes.c_int
     L.amss_lousto_vjp.argtypes = [_IP, _DP, _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]

@@ -127,6 +127,15 @@ class Engine:
     def run_graph(self, level, dt, nsteps, replays=1):
         check(lib().amss_engine_run_graph(self._h, level, dt, nsteps, replays), "amss_engine_run_graph")
 
+    def constraint_norms(self, level):
+        """L2 norms of the Hamiltonian, momentum (x, y, z) and Gamma (x, y, z)
+        constraints and of Theta (Z4c; 0 for BSSN) of a level's current state
+        (Parallel::L2Norm, Parallel.C:4214-4243), as a float64 array of 8."""
+        out = np.zeros(8)
+        check(lib().amss_engine_constraint_norms(self._h, level, out.ctypes.data_as(_DP)),
+              "amss_engine_constraint_norms")
+        return out
+
     def sync(self):
         """Waits for the engine's stream; returns 1 if a NaN was seen."""
         return check(lib().amss_engine_sync(self._h), "amss_engine_sync")

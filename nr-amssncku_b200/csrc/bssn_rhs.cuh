@@ -720,14 +720,18 @@ __device__ __forceinline__ unsigned bssn_rhs_point(const P& q, const Coefs<T>& C
   }
 
   if constexpr (AUX) {
-    double* gm = aux.gamma + q.p;
     const long long s = aux.fs;
-    gm[0] = Gamxxx; gm[s] = Gamxxy; gm[2 * s] = Gamxxz; gm[3 * s] = Gamxyy; gm[4 * s] = Gamxyz; gm[5 * s] = Gamxzz;
-    gm[6 * s] = Gamyxx; gm[7 * s] = Gamyxy; gm[8 * s] = Gamyxz; gm[9 * s] = Gamyyy; gm[10 * s] = Gamyyz;
-    gm[11 * s] = Gamyzz; gm[12 * s] = Gamzxx; gm[13 * s] = Gamzxy; gm[14 * s] = Gamzxz; gm[15 * s] = Gamzyy;
-    gm[16 * s] = Gamzyz; gm[17 * s] = Gamzzz;
-    double* rc = aux.ricci + q.p;
-    rc[0] = Rxx; rc[s] = Rxy; rc[2 * s] = Rxz; rc[3 * s] = Ryy; rc[4 * s] = Ryz; rc[5 * s] = Rzz;
+    if (aux.gamma) {   // the constraint monitor asks for the residuals only
+      double* gm = aux.gamma + q.p;
+      gm[0] = Gamxxx; gm[s] = Gamxxy; gm[2 * s] = Gamxxz; gm[3 * s] = Gamxyy; gm[4 * s] = Gamxyz; gm[5 * s] = Gamxzz;
+      gm[6 * s] = Gamyxx; gm[7 * s] = Gamyxy; gm[8 * s] = Gamyxz; gm[9 * s] = Gamyyy; gm[10 * s] = Gamyyz;
+      gm[11 * s] = Gamyzz; gm[12 * s] = Gamzxx; gm[13 * s] = Gamzxy; gm[14 * s] = Gamzxz; gm[15 * s] = Gamzyy;
+      gm[16 * s] = Gamzyz; gm[17 * s] = Gamzzz;
+    }
+    if (aux.ricci) {
+      double* rc = aux.ricci + q.p;
+      rc[0] = Rxx; rc[s] = Rxy; rc[2 * s] = Rxz; rc[3 * s] = Ryy; rc[4 * s] = Ryz; rc[5 * s] = Rzz;
+    }
     if (aux.co == 0) {
       // :1047-1075 Hamiltonian constraint
       double* o = aux.cons + q.p;

@@ -41,6 +41,10 @@ template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
                          int grid, cudaStream_t s);
 cudaError_t launch_enforce(long long n, long long fs, double* g, double* a, cudaStream_t s);
+template <typename T>
+cudaError_t launch_constraints(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm,
+                               const int* region, double* cons, long long dfs, double* part, int grid,
+                               cudaStream_t s);
 cudaError_t launch_amr_sync(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles, int which,
                             bool fp32_stages, unsigned* status, cudaStream_t s);
 cudaError_t launch_amr_prolong(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
@@ -105,6 +109,7 @@ struct EBlock {
   double bbox[6], pbbox[6];
   std::vector<double> X, Y, Z;
   int face_mask = 0, lowsym = 0;
+  bool l2_by_bbox = false;      // added by bbox: its L2-norm cells follow l2normhelper's bbox test
   double* dX = nullptr;
   double* tl[3] = {nullptr, nullptr, nullptr};
   double* K = nullptr;
@@ -144,6 +149,7 @@ struct ELevel {
   DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
   int nditems = 0;
   long long dfs = 0;            // slot stride of D for this level
+  int* dregion = nullptr;       // per table block: local [lo, hi) of its owned cells inside its patch
   int cur = 0;                  // host mirror of the ring index
   long long steps = 0;
 };
@@ -172,6 +178,9 @@ struct amss_engine {
   bool committed = false;
   int sm_count = 148;
   int nf = NFIELDS_BSSN;        // evolved fields: 24 (BSSN) or 25 (Z4c)
+  double* cons = nullptr;       // constraint residuals of a level (7 x its D stride), grow-only
+  long long cons_cap = 0;
+  double* cpart = nullptr;      // per-CTA partial sums of the constraint norms (8 each)
 };
 
 extern "C" const char* amss_last_error(void) { return g_err.c_str(); }
@@ -214,6 +223,7 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.dti_tiles) cudaFree(L.dti_tiles);
     if (L.ditems) cudaFree(L.ditems);
     if (L.dfaces) cudaFree(L.dfaces);
+    if (L.dregion) cudaFree(L.dregion);
     L.sync.release();
     L.restrict_.release();
     L.prolong.release();
@@ -223,6 +233,8 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
   if (e->dlvl) cudaFree(e->dlvl);
   if (e->arena) cudaFree(e->arena);
   if (e->dstatus) cudaFree(e->dstatus);
+  if (e->cons) cudaFree(e->cons);
+  if (e->cpart) cudaFree(e->cpart);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -261,6 +273,7 @@ extern "C" int amss_engine_add_block(amss_engine* e, int level, const int ex[3],
   p.blocks.push_back((int)e->blocks.size());
   e->patches.push_back(p);
   b.patch = pid;
+  b.l2_by_bbox = true;
   finish_block(e, b, bbox, patch_bbox);
   e->blocks.push_back(b);
   e->levels[level].blocks.push_back((int)e->blocks.size() - 1);
@@ -398,6 +411,35 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     }
   }
   L.ntiles = (int)tiles.size();
+  {
+    // constraint-norm region of each table block, in array indices.  A block
+    // added by bbox: 3 ghost cells off each side, unless the side's outer cell
+    // lies within one cell of the patch box (l2normhelper, fmisc.f90:1286-1303).
+    // An AMR block: its owned cells inside its patch, buffer cells included
+    // (the patch box of Parallel::L2Norm holds them, MPatch.C:48-51).
+    std::vector<int> reg(6 * L.blocks.size());
+    for (size_t m = 0; m < L.blocks.size(); ++m) {
+      const EBlock& b = e->blocks[L.blocks[m]];
+      if (b.l2_by_bbox) {
+        const std::vector<double>* xs[3] = {&b.X, &b.Y, &b.Z};
+        for (int d = 0; d < 3; ++d) {
+          const std::vector<double>& x = *xs[d];
+          const double h = x[1] - x[0];
+          reg[6 * m + d] = std::fabs(x[0] - b.pbbox[d]) < h ? 0 : 3;
+          reg[6 * m + 3 + d] = std::fabs(x[b.ex[d] - 1] - b.pbbox[3 + d]) < h ? b.ex[d] : b.ex[d] - 3;
+        }
+        continue;
+      }
+      Box r = intersect(b.own, e->patches[b.patch].ext());
+      for (int d = 0; d < 3; ++d) {
+        reg[6 * m + d] = r.lo[d] - b.org[d];
+        reg[6 * m + 3 + d] = r.hi[d] - b.org[d];
+      }
+    }
+    if (L.dregion) cudaFree(L.dregion);
+    AMSS_CK(cudaMalloc(&L.dregion, reg.size() * sizeof(int)));
+    AMSS_CK(cudaMemcpy(L.dregion, reg.data(), reg.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   L.dfs = doff;
   L.nditems = (int)items.size();
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
@@ -826,4 +868,39 @@ extern "C" long long amss_engine_level_points(amss_engine* e, int level) {
   long long n = 0;
   for (int b : it->second.blocks) n += e->blocks[b].npts;
   return n;
+}
+
+extern "C" int amss_engine_constraint_norms(amss_engine* e, int level, double* norms) {
+  if (!e || !norms) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms: null argument");
+  if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_constraint_norms: commit the engine first");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms: no such level");
+  ELevel& L = it->second;
+  constexpr int kGrid = 148 * 2;
+  if (e->cons_cap < 7 * L.dfs) {
+    if (e->cons) cudaFree(e->cons);
+    e->cons = nullptr;
+    e->cons_cap = 0;
+    AMSS_CK(cudaMalloc(&e->cons, (size_t)7 * L.dfs * sizeof(double)));
+    e->cons_cap = 7 * L.dfs;
+  }
+  if (!e->cpart) AMSS_CK(cudaMalloc(&e->cpart, (size_t)kGrid * 8 * sizeof(double)));
+  const int tile_pts = e->prm.kernel == 0 ? (int)kPointwiseTile : 128;
+  const cudaError_t err =
+      e->prm.precision == 1
+          ? launch_constraints<float>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, L.dregion, e->cons, L.dfs,
+                                      e->cpart, kGrid, e->stream)
+          : launch_constraints<double>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, L.dregion, e->cons, L.dfs,
+                                       e->cpart, kGrid, e->stream);
+  AMSS_CK(err);
+  e->launches += 2;
+  std::vector<double> part((size_t)kGrid * 8);
+  AMSS_CK(cudaMemcpyAsync(part.data(), e->cpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  for (int c = 0; c < 8; ++c) {
+    double v = 0.0;
+    for (int g = 0; g < kGrid; ++g) v += part[(size_t)g * 8 + c];   // fixed order: reproducible
+    norms[c] = std::sqrt(v);
+  }
+  return 0;
 }

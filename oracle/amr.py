@@ -198,16 +198,17 @@ class OracleHierarchy:
 def grid_noise(level, field, gi, gj, gk, seed):
     """Uniform noise in [-1, 1) as a function of (seed, level, field, global
     cell index) only, so every copy of a cell (owner, ghost, buffer) agrees.
-    splitmix64 finaliser over the packed key."""
-    key = (np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
-           ^ (np.uint64(level) << np.uint64(56)) ^ (np.uint64(field) << np.uint64(48))
-           ^ ((gk.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(32))
-           ^ ((gj.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(16))
-           ^ (gi.astype(np.uint64) & np.uint64(0xFFFF)))
-    z = key + np.uint64(0x9E3779B97F4A7C15)
-    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-    z = z ^ (z >> np.uint64(31))
+    splitmix64 finaliser over the packed key (64-bit wrap-around intended)."""
+    with np.errstate(over="ignore"):
+        key = (np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
+               ^ (np.uint64(level) << np.uint64(56)) ^ (np.uint64(field) << np.uint64(48))
+               ^ ((gk.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(32))
+               ^ ((gj.astype(np.uint64) & np.uint64(0xFFFF)) << np.uint64(16))
+               ^ (gi.astype(np.uint64) & np.uint64(0xFFFF)))
+        z = key + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
     return (z >> np.uint64(11)).astype(np.float64) * (2.0 / 2.0 ** 53) - 1.0
 
 

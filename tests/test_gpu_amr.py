@@ -88,3 +88,106 @@ def test_mixed_amr_error_bound(fp64_reference):
     got = _run_engine(H, init, dt0, 2, precision="mixed")
     errs = _errs(got, ref)
     assert errs.max() <= 1e-6, errs
+
+
+# ---- constraint monitor (Parallel::L2Norm, Parallel.C:4214-4243) -----------
+
+import oracle as O
+
+
+def _oracle_level_norms(H, states, level):
+    """sqrt(sum c^2 dV) over the owned cells of the level's blocks inside their
+    patch (buffer included), residuals from the oracle's compute_rhs_bssn co=0."""
+    sums = np.zeros(7)
+    for i, b in enumerate(H.blocks):
+        if b.level != level:
+            continue
+        X, Y, Z = H.coords(b)
+        cons = O.compute_rhs_bssn(X, Y, Z, states[i], co=0, eps=0.1)[4]
+        p = H.levels[level][b.patch]
+        lo = [max(b.own_lo[d], p.ext_lo[d]) - b.org[d] for d in range(3)]
+        hi = [min(b.own_hi[d], p.ext_hi[d]) - b.org[d] for d in range(3)]
+        c = cons[:, lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+        dv = (X[1] - X[0]) * (Y[1] - Y[0]) * (Z[1] - Z[0])
+        sums += (c * c).sum(axis=(1, 2, 3)) * dv
+    return np.sqrt(sums)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_constraint_norms_match_oracle(precision):
+    H = small_hierarchy()
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=1e-6)
+    e = amss_b200.Engine.from_hierarchy(H, precision=precision, eps=0.1)
+    for i, st in enumerate(init):
+        e.set_state(i, st)
+    e.coarse_step(0.25 * H.h0)
+    assert e.sync() == 0
+    states = [e.get_state(i) for i in range(len(H.blocks))]
+    for lv in range(len(H.levels)):
+        got = e.constraint_norms(lv)
+        ref = _oracle_level_norms(H, states, lv)
+        assert np.all(ref > 0)
+        np.testing.assert_allclose(got[:7], ref, rtol=1e-12, atol=0)
+        assert got[7] == 0.0
+    e.close()
+
+
+def test_z4c_constraint_norms_match_oracle():
+    """Z4c: the residuals of the first 24 fields (constraint_bssn) plus the
+    L2 norm of Theta (Z4c_class.C:2491-2510)."""
+    H = small_hierarchy()
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=1e-6, nf=25)
+    e = amss_b200.Engine.from_hierarchy(H, precision="fp64", eps=0.1, formulation="z4c")
+    for i, st in enumerate(init):
+        e.set_state(i, st)
+    e.coarse_step(0.25 * H.h0)
+    assert e.sync() == 0
+    states = [e.get_state(i) for i in range(len(H.blocks))]
+    for lv in range(len(H.levels)):
+        got = e.constraint_norms(lv)
+        ref = _oracle_level_norms(H, [np.ascontiguousarray(s[:24]) for s in states], lv)
+        np.testing.assert_allclose(got[:7], ref, rtol=1e-12, atol=0)
+        th = 0.0
+        for i, b in enumerate(H.blocks):
+            if b.level != lv:
+                continue
+            p = H.levels[lv][b.patch]
+            lo = [max(b.own_lo[d], p.ext_lo[d]) - b.org[d] for d in range(3)]
+            hi = [min(b.own_hi[d], p.ext_hi[d]) - b.org[d] for d in range(3)]
+            t = states[i][24, lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+            X, Y, Z = H.coords(b)
+            th += float((t * t).sum()) * (X[1] - X[0]) * (Y[1] - Y[0]) * (Z[1] - Z[0])
+        assert th > 0
+        np.testing.assert_allclose(got[7], np.sqrt(th), rtol=1e-12, atol=0)
+    e.close()
+
+
+def test_constraint_norms_bbox_blocks():
+    """Two blocks added by bbox inside one patch box, overlapping by 3 ghost
+    cells: l2normhelper's bbox test (fmisc.f90:1286-1303) drops the ghosts of
+    the shared side only."""
+    n, h, lo = 24, 0.25, -3.0
+    hi = lo + n * h
+    mid = lo + 12 * h
+    pbox = (lo, lo, lo, hi, hi, hi)
+    boxes = [(lo, lo, lo, mid + 3 * h, hi, hi), (mid - 3 * h, lo, lo, hi, hi, hi)]
+    e = amss_b200.Engine(precision="fp64", eps=0.1)
+    sums = np.zeros(7)
+    rng = np.random.default_rng(7)
+    for bb in boxes:
+        ex = (15, n, n)
+        e.add_block(0, ex, bb, pbox)
+    e.commit()
+    for bid, bb in enumerate(boxes):
+        X = bb[0] + (np.arange(15) + 0.5) * h
+        Y = lo + (np.arange(n) + 0.5) * h
+        st = amss_b200.dropin.get_lousto_nbhs(X, Y, Y, [1.0], [[0.3, -0.2, 0.1]])
+        st += 1e-6 * rng.uniform(-1, 1, st.shape)
+        e.set_state(bid, st)
+        cons = O.compute_rhs_bssn(X, Y, Y, st, co=0, eps=0.1)[4]
+        i0, i1 = (0, 12) if bid == 0 else (3, 15)
+        c = cons[:, :, :, i0:i1]
+        sums += (c * c).sum(axis=(1, 2, 3)) * h ** 3
+    got = e.constraint_norms(0)
+    e.close()
+    np.testing.assert_allclose(got[:7], np.sqrt(sums), rtol=1e-12, atol=0)
