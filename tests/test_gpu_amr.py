@@ -162,32 +162,57 @@ def test_z4c_constraint_norms_match_oracle():
     e.close()
 
 
-def test_constraint_norms_bbox_blocks():
+@pytest.mark.parametrize("symmetry", [0, 1])
+def test_constraint_norms_bbox_blocks(symmetry):
     """Two blocks added by bbox inside one patch box, overlapping by 3 ghost
     cells: l2normhelper's bbox test (fmisc.f90:1286-1303) drops the ghosts of
-    the shared side only."""
+    the shared side only.  Symmetry 1: the blocks start at the z = 0 plane
+    (mirrored stencils, the plane's cells counted)."""
     n, h, lo = 24, 0.25, -3.0
     hi = lo + n * h
     mid = lo + 12 * h
-    pbox = (lo, lo, lo, hi, hi, hi)
-    boxes = [(lo, lo, lo, mid + 3 * h, hi, hi), (mid - 3 * h, lo, lo, hi, hi, hi)]
-    e = amss_b200.Engine(precision="fp64", eps=0.1)
+    zlo = 0.0 if symmetry else lo
+    zhi = zlo + n * h
+    pbox = (lo, lo, zlo, hi, hi, zhi)
+    boxes = [(lo, lo, zlo, mid + 3 * h, hi, zhi), (mid - 3 * h, lo, zlo, hi, hi, zhi)]
+    e = amss_b200.Engine(precision="fp64", eps=0.1, symmetry=symmetry)
     sums = np.zeros(7)
     rng = np.random.default_rng(7)
     for bb in boxes:
-        ex = (15, n, n)
-        e.add_block(0, ex, bb, pbox)
+        e.add_block(0, (15, n, n), bb, pbox)
     e.commit()
+    Y = lo + (np.arange(n) + 0.5) * h
+    Z = zlo + (np.arange(n) + 0.5) * h
     for bid, bb in enumerate(boxes):
         X = bb[0] + (np.arange(15) + 0.5) * h
-        Y = lo + (np.arange(n) + 0.5) * h
-        st = amss_b200.dropin.get_lousto_nbhs(X, Y, Y, [1.0], [[0.3, -0.2, 0.1]])
+        st = amss_b200.dropin.get_lousto_nbhs(X, Y, Z, [1.0], [[0.3, -0.2, 0.1]])
         st += 1e-6 * rng.uniform(-1, 1, st.shape)
         e.set_state(bid, st)
-        cons = O.compute_rhs_bssn(X, Y, Y, st, co=0, eps=0.1)[4]
+        cons = O.compute_rhs_bssn(X, Y, Z, st, symmetry=symmetry, co=0, eps=0.1)[4]
         i0, i1 = (0, 12) if bid == 0 else (3, 15)
         c = cons[:, :, :, i0:i1]
         sums += (c * c).sum(axis=(1, 2, 3)) * h ** 3
     got = e.constraint_norms(0)
     e.close()
     np.testing.assert_allclose(got[:7], np.sqrt(sums), rtol=1e-12, atol=0)
+
+
+def test_hamiltonian_norm_converges_at_fourth_order():
+    """Brill-Lindquist data (the exact solution, H = 0) on [2, 6]^3 away from
+    the puncture at two resolutions: the monitor's Hamiltonian norm falls by
+    2^4 per doubling.  Each block sits inside a larger patch box, so its 3
+    ghost cells are left out and both norms cover exactly [2, 6]^3."""
+    norms = []
+    for cells in (16, 32):
+        h = 4.0 / cells
+        ex = cells + 6
+        bb = (2.0 - 3 * h,) * 3 + (6.0 + 3 * h,) * 3
+        e = amss_b200.Engine(precision="fp64", eps=0.1)
+        e.add_block(0, (ex, ex, ex), bb, (-10.0,) * 3 + (10.0,) * 3)
+        e.commit()
+        X = bb[0] + (np.arange(ex) + 0.5) * h
+        e.set_state(0, amss_b200.dropin.get_lousto_nbhs(X, X, X, [1.0], [[0.0, 0.0, 0.0]]))
+        norms.append(e.constraint_norms(0)[0])
+        e.close()
+    order = np.log2(norms[0] / norms[1])
+    assert 3.7 < order < 4.3, (norms, order)
