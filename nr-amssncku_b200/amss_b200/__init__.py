@@ -3,13 +3,15 @@
 `dropin` mirrors the reference's per-block Fortran kernel calls; `engine` is
 the batched device-resident level step; `adjoint` differentiates a block's
 evolution (torch.autograd.Function); `initial` builds puncture initial data
-on hierarchies.  All run only on a CUDA device.
+on hierarchies; `monitor` writes the constraint output file.  All compute runs
+only on a CUDA device.
 """
 from ._lib import AmssError, lib, last_error, header_functions  # noqa: F401
-from . import dropin, engine, initial  # noqa: F401
+from . import dropin, engine, initial, monitor  # noqa: F401
 from .engine import Engine  # noqa: F401
 
-__all__ = ["AmssError", "lib", "last_error", "header_functions", "dropin", "engine", "initial", "Engine"]
+__all__ = ["AmssError", "lib", "last_error", "header_functions", "dropin", "engine", "initial", "monitor",
+           "Engine"]
 
 
 def __getattr__(name):

@@ -1,0 +1,73 @@
+"""The constraint output file of an evolution (bssn_constraint.dat), written
+from the engine's constraint monitor.
+
+File format and cadence follow the reference:
+
+* monitor::monitor (monitor.C:15-101): the file is <out_dir>/<name>; when it
+  exists already (a run restarted from a checkpoint) the name becomes
+  1_<name>, 2_<name>, ... (monitor.C:79-86).  Three header lines: "# File
+  created on " + asctime() (which ends in a newline), "#", and the column
+  header "# time Ham Px Py Pz Gx Gy Gz" (bssn_class.C:100-103).
+* monitor::writefile (monitor.C:137-150): iostream with setprecision(8), the
+  default float format (that is printf's %.8g) and ios::left set by the
+  constructor: the time in a field of 14, then per value a blank and a field
+  of 15, one line per call.
+* bssn_class::Constraint_Out (bssn_class.C:7296-7300, 7472-7505): every call
+  adds the coarse step dT * 0.5^max(0, trfls) to LastConsOut; once that reaches
+  AnasTime, one line per level (levels in order, all at the same PhysTime) with
+  the 7 norms of Parallel::L2Norm, and LastConsOut goes back to 0.  A Z4c run
+  writes 8 values per line, Theta's norm last (Z4c_class.C:2502-2511).
+"""
+import os
+import time
+
+HEADER = "# time Ham Px Py Pz Gx Gy Gz"
+
+
+def format_line(t, values):
+    """One monitor::writefile line (without the newline)."""
+    return "%-14.8g" % t + "".join(" %-15.8g" % v for v in values)
+
+
+def open_name(out_dir, name):
+    """monitor.C:79-86: the first of name, 1_name, 2_name, ... that does not exist."""
+    path = os.path.join(out_dir, name)
+    i = 1
+    while os.path.exists(path):
+        path = os.path.join(out_dir, f"{i}_{name}")
+        i += 1
+    return path
+
+
+class ConstraintMonitor:
+    """bssn_constraint.dat for an engine.  `anas_time` is the output
+    interval (AnasTime), `trfls` the level below which there is no time
+    refinement (0 on the engine's hierarchies), `z4c` adds Theta's column."""
+
+    def __init__(self, out_dir, anas_time, name="bssn_constraint.dat", trfls=0, z4c=False):
+        self.path = open_name(out_dir, name)
+        self.anas_time = float(anas_time)
+        self.trfls = int(trfls)
+        self.nvals = 8 if z4c else 7
+        self.last = 0.0   # LastConsOut
+        with open(self.path, "w") as f:
+            f.write("# File created on " + time.asctime() + "\n")
+            f.write("#\n")
+            f.write(HEADER + "\n")
+
+    def write(self, engine, phys_time, nlevels):
+        """One line per level of the engine's current state at phys_time."""
+        with open(self.path, "a") as f:
+            for lv in range(nlevels):
+                c = engine.constraint_norms(lv)
+                f.write(format_line(phys_time, c[:self.nvals]) + "\n")
+
+    def after_step(self, engine, phys_time, dT, nlevels):
+        """Constraint_Out after a coarse step of dT ending at phys_time;
+        returns True when it wrote."""
+        self.last += dT * 0.5 ** max(0, self.trfls)
+        if self.last >= self.anas_time:
+            self.write(engine, phys_time, nlevels)
+            self.last = 0.0
+            return True
+        return False
