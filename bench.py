@@ -202,6 +202,7 @@ def run_ours(args, rank, world):
                                           formulation=args.formulation)
     for i, st in enumerate(init):
         eng.set_state(i, st)
+    eng.set_punctures(w["pos"])   # Step tracks the punctures on the finest level (MAPBH 0)
     stream = torch.cuda.ExternalStream(eng.stream)
 
     # warm-up, then K timed steps bracketed by a barrier + synchronize
@@ -225,6 +226,7 @@ def run_ours(args, rank, world):
         ev1.synchronize()
     nan = eng.sync()
     torch.cuda.synchronize()
+    tracked = eng.punctures().tolist()   # fails if a puncture left the finest level
     ms = ev0.elapsed_time(ev1)
     launches = eng.launches - launches0
     ms = max_over_ranks(ms, world)
@@ -276,6 +278,8 @@ def run_ours(args, rank, world):
                    "precision": args.precision, "kernel": args.kernel, "graph": bool(args.graph),
                    "zone_updates_per_step_per_gpu": zones, "point_updates_per_step": npts,
                    "levels": len(H.levels), "blocks": len(H.blocks),
+                   "puncture_tracking": f"{len(w['pos'])} punctures on the finest level, every substep, "
+                                        "inside the step",
                    "l2": "state + stages + K of the hierarchy (GBs) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{world} (no data-path collective)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -291,6 +295,7 @@ def run_ours(args, rank, world):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "nan": bool(nan),
+        "punctures_after_warmup_and_timed_steps": tracked,
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w, init)

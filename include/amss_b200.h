@@ -283,6 +283,37 @@ long long amss_engine_launch_count(amss_engine* e);
  * buffer cells included.  Waits for the engine's stream. */
 int amss_engine_constraint_norms(amss_engine* e, int level, double norms[8]);
 
+/* Values of fields at points of one level (Parallel::PatList_Interp_Points,
+ * Parallel.C:5614-5667, with Patch::Interp_Points, MPatch.C:339-500, and
+ * global_interp, fmisc.f90:712-794: 6-point Lagrange per axis by Neville's
+ * scheme, z then y then x, mirrored cells times the field's parity at a
+ * symmetry plane).  xyz: npts points (x, y, z); fields: nvar state indices;
+ * soa: 3 parities per field (NULL: all +1); out: npts x nvar.  found[p]
+ * (may be NULL) is 0 when no patch of the level holds point p -- the
+ * reference's `false`, on which compute_Porg_rhs (bssn_class.C:6879-6932)
+ * tries the next coarser level -- and its values are 0.  A point inside a
+ * patch but in none of its blocks, or a stencil that leaves its block, is
+ * AMSS_ERR_ARG.  Reads the current state; waits for the engine's stream. */
+int amss_engine_interp_points(amss_engine* e, int level, int npts, const double* xyz, int nvar, const int* fields,
+                              const double* soa, double* out, int* found);
+
+/* Puncture tracking (bssn_class::Step with MAPBH 0: bssn_class.C:3360-3390,
+ * :3730-3760, :3804-3812, :3890-3898; compute_Porg_rhs, :6879-6932;
+ * rungekutta4_scalar, rungekutta4_rout.f90:6-47).  n <= 10 positions
+ * (x, y, z) = Porg0; from then on every step of the finest level also
+ * advances them on the device: at each RK4 substep minus the shift of the
+ * substep's input state, interpolated as amss_engine_interp_points does,
+ * drives a scalar RK4 (|z| kept with Symmetry > 0, |x|, |y| with Symmetry 2).
+ * The mixed form reads the shift of its FP32 stages; n = 0 stops tracking.
+ * The reference tries coarser levels when a puncture leaves the finest one;
+ * the engine flags it instead, and amss_engine_get_punctures then fails with
+ * AMSS_ERR_STATE. */
+int amss_engine_set_punctures(amss_engine* e, int n, const double* pos);
+
+/* The tracked positions (3 n doubles) after the steps issued so far; waits
+ * for the engine's stream. */
+int amss_engine_get_punctures(amss_engine* e, double* pos);
+
 /* ---- Adjoint of a single-patch BSSN evolution (no reference counterpart:
  * the reference has no derivative code; the forward it differentiates is the
  * level-0 RK4 step of bssn_class::Step, bssn_class.C:2981-3700, with

@@ -59,6 +59,10 @@ def lib():
     L.amss_engine_launch_count.argtypes = [ctypes.c_void_p]
     L.amss_engine_launch_count.restype = ctypes.c_longlong
     L.amss_engine_constraint_norms.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+    L.amss_engine_set_punctures.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+    L.amss_engine_get_punctures.argtypes = [ctypes.c_void_p, _DP]
+    L.amss_engine_interp_points.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP, ctypes.c_int, _IP, _DP,
+                                            _DP, _IP]
     L.get_lousto_nbhs_.restype = ctypes.c_int
     L.amss_lousto_vjp.restype = ctypes.c_int
     L.amss_lousto_vjp.argtypes = [_IP, _DP, _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]

@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import _DP, AmssError, check, last_error, lib
+from ._lib import _DP, _IP, AmssError, check, last_error, lib
 
 
 class _Params(ctypes.Structure):
@@ -38,6 +38,7 @@ class Engine:
         if not self._h:
             raise AmssError("amss_engine_create failed: " + last_error())
         self.blocks = []
+        self._ntrack = 0
 
     def close(self):
         if self._h:
@@ -134,6 +135,38 @@ class Engine:
         out = np.zeros(8)
         check(lib().amss_engine_constraint_norms(self._h, level, out.ctypes.data_as(_DP)),
               "amss_engine_constraint_norms")
+        return out
+
+    def interp_points(self, level, points, fields, soa=None):
+        """Values of state fields at points of a level (Parallel::PatList_Interp_Points,
+        Parallel.C:5614-5667): points (n, 3), fields a list of state indices,
+        soa their parities (nvar, 3) or None for all +1.  Returns
+        (values (n, nvar), found (n,) bool); points outside every patch of
+        the level are not found and read 0."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        fl = np.ascontiguousarray(fields, dtype=np.int32).reshape(-1)
+        out = np.zeros((pts.shape[0], fl.size))
+        found = np.zeros(pts.shape[0], dtype=np.int32)
+        sp = None
+        if soa is not None:
+            sa = np.ascontiguousarray(soa, dtype=np.float64).reshape(fl.size, 3)
+            sp = sa.ctypes.data_as(_DP)
+        check(lib().amss_engine_interp_points(self._h, level, pts.shape[0], pts.ctypes.data_as(_DP), fl.size,
+                                              fl.ctypes.data_as(_IP), sp, out.ctypes.data_as(_DP),
+                                              found.ctypes.data_as(_IP)), "amss_engine_interp_points")
+        return out, found.astype(bool)
+
+    def set_punctures(self, positions):
+        """Track punctures (n, 3) on the finest level from now on (FP64 engines)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        self._ntrack = pos.shape[0]
+        check(lib().amss_engine_set_punctures(self._h, pos.shape[0], pos.ctypes.data_as(_DP)),
+              "amss_engine_set_punctures")
+
+    def punctures(self):
+        """The tracked positions (n, 3) after the steps issued so far."""
+        out = np.zeros((self._ntrack, 3))
+        check(lib().amss_engine_get_punctures(self._h, out.ctypes.data_as(_DP)), "amss_engine_get_punctures")
         return out
 
     def sync(self):

@@ -24,6 +24,7 @@
 #include "amr_types.cuh"
 #include "deriv.cuh"
 #include "dev_util.cuh"
+#include "interp.cuh"
 
 namespace amss {
 
@@ -181,6 +182,14 @@ struct amss_engine {
   double* cons = nullptr;       // constraint residuals of a level (7 x its D stride), grow-only
   long long cons_cap = 0;
   double* cpart = nullptr;      // per-CTA partial sums of the constraint norms (8 each)
+  int ntrack = 0, track_level = -1;   // puncture tracking on the finest level
+  TrackState* dtrack = nullptr;
+  TrackPatch* dtpatch = nullptr;
+  TrackBlock* dtblock = nullptr;
+  int ntpatch = 0;
+  InterpItem* iitems = nullptr;   // point interpolation: items and results, grow-only
+  double* iout = nullptr;
+  long long icap = 0;
 };
 
 extern "C" const char* amss_last_error(void) { return g_err.c_str(); }
@@ -235,6 +244,11 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
   if (e->dstatus) cudaFree(e->dstatus);
   if (e->cons) cudaFree(e->cons);
   if (e->cpart) cudaFree(e->cpart);
+  if (e->iitems) cudaFree(e->iitems);
+  if (e->dtrack) cudaFree(e->dtrack);
+  if (e->dtpatch) cudaFree(e->dtpatch);
+  if (e->dtblock) cudaFree(e->dtblock);
+  if (e->iout) cudaFree(e->iout);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -699,9 +713,15 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
   e->launches++;
   const bool split = e->prm.kernel == 0;
   const int dgrid = std::min(L.nditems, e->sm_count * 16);
+  const bool track = e->ntrack > 0 && level == e->track_level;
   for (int sub = 0; sub < 4; ++sub) {
     cudaError_t err;
     const int enf = sub < 3 ? 1 : 0;
+    if (track) {   // the substep's input state is complete (U0, or the synced stage)
+      AMSS_CK(launch_track(e->dtpatch, e->ntpatch, e->dtblock, e->dlvl + 2 * level, e->dtrack, e->ntrack, sub, dt,
+                           e->prm.symmetry, e->stream));
+      e->launches++;
+    }
     if (split) {
       const cudaError_t ed = mixed ? launch_deriv<float, float>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream)
                                    : launch_deriv<double, double>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream);
@@ -902,5 +922,231 @@ extern "C" int amss_engine_constraint_norms(amss_engine* e, int level, double* n
     for (int g = 0; g < kGrid; ++g) v += part[(size_t)g * 8 + c];   // fixed order: reproducible
     norms[c] = std::sqrt(v);
   }
+  return 0;
+}
+
+// The patches of a level as Parallel::PatList_Interp_Points walks them:
+// engine patches in order; blocks added by bbox grouped by their patch box.
+struct IPatch {
+  int patch;           // engine patch, -1 for a group of blocks added by bbox
+  double pbb[6], h[3];
+  int buffer;
+  std::vector<int> blocks;
+};
+
+static std::vector<IPatch> level_patches(amss_engine* e, const ELevel& L) {
+  std::vector<IPatch> ps;
+  for (int bid : L.blocks) {
+    const EBlock& b = e->blocks[bid];
+    IPatch* g = nullptr;
+    for (auto& q : ps)
+      if ((b.l2_by_bbox && q.patch < 0 && std::memcmp(q.pbb, b.pbbox, sizeof q.pbb) == 0) ||
+          (!b.l2_by_bbox && q.patch == b.patch))
+        g = &q;
+    if (!g) {
+      IPatch q;
+      q.patch = b.l2_by_bbox ? -1 : b.patch;
+      std::memcpy(q.pbb, b.pbbox, sizeof q.pbb);
+      q.buffer = b.l2_by_bbox ? 0 : e->patches[b.patch].buffer;
+      for (int d = 0; d < 3; ++d) {
+        long long shape;
+        if (b.l2_by_bbox) {
+          const double hb = (b.bbox[3 + d] - b.bbox[d]) / b.ex[d];
+          shape = std::llround((b.pbbox[3 + d] - b.pbbox[d]) / hb);
+        } else {
+          const Box x = e->patches[b.patch].ext();
+          shape = x.hi[d] - x.lo[d];
+        }
+        q.h[d] = (q.pbb[3 + d] - q.pbb[d]) / (double)shape;   // Patch::getdX
+      }
+      ps.push_back(q);
+      g = &ps.back();
+    }
+    g->blocks.push_back(bid);
+  }
+  return ps;
+}
+
+// Patch::Interp_Points' box of a block (Cell): less the buffer on a side it
+// shares with the patch box, else less the ghosts.
+static void find_box(const EBlock& b, const IPatch& q, double lo[3], double hi[3]) {
+  for (int d = 0; d < 3; ++d) {
+    const double h = q.h[d];
+    lo[d] = std::fabs(b.bbox[d] - q.pbb[d]) < h / 2 ? b.bbox[d] + q.buffer * h : b.bbox[d] + 3 * h;
+    hi[d] = std::fabs(b.bbox[3 + d] - q.pbb[3 + d]) < h / 2 ? b.bbox[3 + d] - q.buffer * h : b.bbox[3 + d] - 3 * h;
+  }
+}
+
+// Point interpolation on a level.  Host side of Parallel::PatList_Interp_Points
+// (Parallel.C:5614-5667) and Patch::Interp_Points (MPatch.C:339-500, Cell):
+// the first patch of the level whose box less its buffer holds the point, then
+// the first block of that patch whose box less its ghosts (less the buffer on
+// a side it shares with the patch box) holds it to half a cell; and the
+// stencil choice of global_interp (fmisc.f90:738-781, ORDN = 6).  Blocks added
+// by bbox form one patch per distinct patch box, with no buffer.
+extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, const double* xyz, int nvar,
+                                         const int* fields, const double* soa, double* out, int* found) {
+  if (!e || (npts > 0 && (!xyz || !out)) || nvar < 1 || !fields)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: null argument or nvar < 1");
+  if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_interp_points: commit the engine first");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: no such level");
+  for (int v = 0; v < nvar; ++v)
+    if (fields[v] < 0 || fields[v] >= e->nf) return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: bad field");
+  if (npts <= 0) return 0;
+  const std::vector<IPatch> ps = level_patches(e, it->second);
+  std::vector<InterpItem> items;
+  std::vector<long long> where;   // output slot of each item
+  for (int p = 0; p < npts; ++p) {
+    const double* pt = xyz + 3 * (long long)p;
+    if (!std::isfinite(pt[0]) || !std::isfinite(pt[1]) || !std::isfinite(pt[2]))
+      return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: a point is not finite");
+    int ok = 0;
+    for (const auto& q : ps) {
+      bool inp = true;
+      for (int d = 0; d < 3; ++d)
+        if (pt[d] < q.pbb[d] + q.buffer * q.h[d] || pt[d] > q.pbb[3 + d] - q.buffer * q.h[d]) inp = false;
+      if (!inp) continue;
+      for (int bid : q.blocks) {
+        const EBlock& b = e->blocks[bid];
+        bool inb = true;
+        double lo[3], hi[3];
+        find_box(b, q, lo, hi);
+        for (int d = 0; d < 3; ++d)
+          if (pt[d] - lo[d] < -q.h[d] / 2 || pt[d] - hi[d] > q.h[d] / 2) inb = false;
+        if (!inb) continue;
+        // global_interp's stencil (fmisc.f90:738-781)
+        const std::vector<double>* co[3] = {&b.X, &b.Y, &b.Z};
+        InterpItem t;
+        for (int d = 0; d < 3; ++d) {
+          const std::vector<double>& c = *co[d];
+          const double dd = c[1] - c[0];
+          const int cxI = (int)((pt[d] - c[0]) / dd + 0.4) + 1;
+          int cxB = cxI - 2, cxT = cxB + 5;
+          const bool mirror = (d < 2 && e->prm.symmetry == 2) || (d == 2 && e->prm.symmetry != 0);
+          const int cmin = mirror && std::fabs(c[0]) < dd ? -2 : 1;
+          if (cxB < cmin) { cxB = cmin; cxT = cxB + 5; }
+          if (cxT > b.ex[d]) { cxT = b.ex[d]; cxB = cxT - 5; }
+          if (cxT > b.ex[d] || (cxB <= 0 && 1 - cxB > b.ex[d]))
+            return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: stencil outside the block (decide3d)");
+          t.ex[d] = b.ex[d];
+          t.cxB[d] = cxB;
+          t.cx[d] = cxB > 0 ? (pt[d] - c[cxB - 1]) / dd : (pt[d] + c[-cxB]) / dd;
+        }
+        const double* u = cur_state(e, b);
+        for (int v = 0; v < nvar; ++v) {
+          t.f = u + (long long)fields[v] * b.fs;
+          for (int d = 0; d < 3; ++d) t.soa[d] = soa ? soa[3 * v + d] : 1.0;
+          items.push_back(t);
+          where.push_back((long long)p * nvar + v);
+        }
+        ok = 1;
+        break;
+      }
+      if (!ok) return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: a point of a patch lies in none of its blocks");
+      break;
+    }
+    if (found) found[p] = ok;
+    if (!ok)
+      for (int v = 0; v < nvar; ++v) out[(long long)p * nvar + v] = 0.0;
+  }
+  const long long n = (long long)items.size();
+  if (n == 0) return 0;
+  if (e->icap < n) {
+    if (e->iitems) cudaFree(e->iitems);
+    if (e->iout) cudaFree(e->iout);
+    e->iitems = nullptr;
+    e->iout = nullptr;
+    e->icap = 0;
+    AMSS_CK(cudaMalloc(&e->iitems, n * sizeof(InterpItem)));
+    AMSS_CK(cudaMalloc(&e->iout, n * sizeof(double)));
+    e->icap = n;
+  }
+  AMSS_CK(cudaMemcpyAsync(e->iitems, items.data(), n * sizeof(InterpItem), cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(launch_interp_points(e->iitems, (int)n, e->iout, e->stream));
+  e->launches++;
+  std::vector<double> res(n);
+  AMSS_CK(cudaMemcpyAsync(res.data(), e->iout, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  for (long long i = 0; i < n; ++i) out[where[i]] = res[i];
+  return 0;
+}
+
+// Puncture tracking (bssn_class::Step with MAPBH 0, bssn_class.C:3360-3390,
+// :3730-3760, :3804-3812, :3890-3898): positions advanced by RK4 with the
+// finest level's substeps, on the device inside the step (and its graphs).
+extern "C" int amss_engine_set_punctures(amss_engine* e, int n, const double* pos) {
+  if (!e || n < 0 || n > kMaxPunctures || (n > 0 && !pos))
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_set_punctures: 0 <= n <= 10 positions");
+  if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_set_punctures: commit the engine first");
+  e->ntrack = 0;
+  if (n == 0) return 0;
+  const int level = e->levels.rbegin()->first;
+  const std::vector<IPatch> ps = level_patches(e, e->levels[level]);
+  std::vector<TrackPatch> tp;
+  std::vector<TrackBlock> tb;
+  for (const auto& q : ps) {
+    TrackPatch P;
+    for (int d = 0; d < 3; ++d) {
+      P.lo[d] = q.pbb[d] + q.buffer * q.h[d];
+      P.hi[d] = q.pbb[3 + d] - q.buffer * q.h[d];
+      P.half[d] = q.h[d] / 2;
+    }
+    P.b0 = (int)tb.size();
+    for (int bid : q.blocks) {
+      const EBlock& b = e->blocks[bid];
+      TrackBlock B;
+      for (int t = 0; t < 3; ++t) B.tl[t] = b.tl[t];
+      B.stage[0] = b.st[0];
+      B.stage[1] = b.st[1];
+      B.f32 = e->prm.precision == 1;
+      B.fs = b.fs;
+      find_box(b, q, B.flo, B.fhi);
+      const std::vector<double>* co[3] = {&b.X, &b.Y, &b.Z};
+      for (int d = 0; d < 3; ++d) {
+        B.ex[d] = b.ex[d];
+        B.blo[d] = b.bbox[d];
+        B.bh[d] = (b.bbox[3 + d] - b.bbox[d]) / b.ex[d];
+        B.x0[d] = (*co[d])[0];
+        B.dd[d] = (*co[d])[1] - (*co[d])[0];
+        const bool mirror = (d < 2 && e->prm.symmetry == 2) || (d == 2 && e->prm.symmetry != 0);
+        B.cmin[d] = mirror && std::fabs(B.x0[d]) < B.dd[d] ? -2 : 1;
+      }
+      tb.push_back(B);
+    }
+    P.b1 = (int)tb.size();
+    tp.push_back(P);
+  }
+  if (e->dtpatch) cudaFree(e->dtpatch);
+  if (e->dtblock) cudaFree(e->dtblock);
+  e->dtpatch = nullptr;
+  e->dtblock = nullptr;
+  AMSS_CK(cudaMalloc(&e->dtpatch, tp.size() * sizeof(TrackPatch)));
+  AMSS_CK(cudaMalloc(&e->dtblock, tb.size() * sizeof(TrackBlock)));
+  if (!e->dtrack) AMSS_CK(cudaMalloc(&e->dtrack, sizeof(TrackState)));
+  TrackState S;
+  std::memset(&S, 0, sizeof S);
+  for (int i = 0; i < 3 * n; ++i) {
+    if (!std::isfinite(pos[i])) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_punctures: a position is not finite");
+    S.p0[i] = S.p[i] = pos[i];
+  }
+  AMSS_CK(cudaMemcpyAsync(e->dtpatch, tp.data(), tp.size() * sizeof(TrackPatch), cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(cudaMemcpyAsync(e->dtblock, tb.data(), tb.size() * sizeof(TrackBlock), cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(cudaMemcpyAsync(e->dtrack, &S, sizeof S, cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  e->ntpatch = (int)tp.size();
+  e->track_level = level;
+  e->ntrack = n;
+  return 0;
+}
+
+extern "C" int amss_engine_get_punctures(amss_engine* e, double* pos) {
+  if (!e || !pos) return amss_fail(AMSS_ERR_ARG, "amss_engine_get_punctures: null argument");
+  if (e->ntrack == 0) return amss_fail(AMSS_ERR_STATE, "amss_engine_get_punctures: no punctures set");
+  TrackState S;
+  AMSS_CK(cudaMemcpyAsync(&S, e->dtrack, sizeof S, cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  for (int i = 0; i < 3 * e->ntrack; ++i) pos[i] = S.p0[i];
+  if (S.err) return amss_fail(AMSS_ERR_STATE, "amss_engine_get_punctures: a puncture left the finest level");
   return 0;
 }

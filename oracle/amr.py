@@ -54,6 +54,50 @@ class OracleHierarchy:
                 X=X, Y=Y, Z=Z, pbbox=np.array(H.patch_bbox(p)), ex=(ctypes.c_int * 3)(*b.ex)))
         self.cur = [0] * len(H.levels)
         self.steps = [0] * len(H.levels)
+        self.porg0 = None   # tracked punctures (set_punctures)
+
+    # puncture tracking -------------------------------------------------------
+    def set_punctures(self, positions):
+        """bssn_class::Step with MAPBH 0 (bssn_class.C:3360-3390, :3730-3760,
+        :3804-3812, :3890-3898): positions advanced with the finest level's
+        substeps by rungekutta4_scalar (rungekutta4_rout.f90:6-47), their
+        right-hand side minus the shift of the substep's input state
+        (compute_Porg_rhs, bssn_class.C:6879-6932) on the finest level."""
+        self.porg0 = [list(map(float, p)) for p in positions]
+        self.porg = [list(p) for p in self.porg0]
+        self.prhs = [[0.0] * 3 for _ in self.porg0]
+
+    def _track(self, level, sub, arrays, dt):
+        import interp as OI
+        states = [None] * len(self.H.blocks)
+        for bi in arrays:
+            states[bi] = arrays[bi]
+        patches = OI.hierarchy_patches(self.H, level, states)
+        src = self.porg0 if sub == 0 else self.porg
+        for n, pos in enumerate([list(p) for p in src]):
+            vals, found = OI.interp_points(patches, [tuple(pos)], [18, 19, 20],
+                                           [(-1, 1, 1), (1, -1, 1), (1, 1, -1)], self.symmetry)
+            if not found[0]:
+                raise ValueError("a puncture left the finest level")
+            for v in range(3):
+                r = -vals[0][v]
+                f0 = self.porg0[n][v]
+                if sub == 0:
+                    self.prhs[n][v] = r
+                    pn = f0 + 0.5 * dt * r
+                elif sub == 1:
+                    self.prhs[n][v] = self.prhs[n][v] + 2.0 * r
+                    pn = f0 + 0.5 * dt * r
+                elif sub == 2:
+                    self.prhs[n][v] = self.prhs[n][v] + 2.0 * r
+                    pn = f0 + dt * r
+                else:
+                    pn = f0 + (1.0 / 6.0) * dt * (r + self.prhs[n][v])
+                if (self.symmetry > 0 and v == 2) or (self.symmetry == 2 and v < 2):
+                    pn = abs(pn)
+                self.porg[n][v] = pn
+        if sub == 3:
+            self.porg0 = [list(p) for p in self.porg]
 
     # state access ------------------------------------------------------------
     def state(self, bi):
@@ -94,7 +138,12 @@ class OracleHierarchy:
         ids = [i for p in self.H.levels[level] for i in p.blocks]
         c = self.cur[level]
         err = 0
+        finest = self.porg0 is not None and level == len(self.H.levels) - 1
         for sub in range(4):
+            if finest:
+                key = {0: None, 1: "A", 2: "B", 3: "A"}[sub]
+                self._track(level, sub, {bi: (self.blk[bi]["U"][c] if key is None else self.blk[bi][key])
+                                         for bi in ids}, dt)
             for bi in ids:
                 d = self.blk[bi]
                 u0 = d["U"][c]

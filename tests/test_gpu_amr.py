@@ -216,3 +216,136 @@ def test_hamiltonian_norm_converges_at_fourth_order():
         e.close()
     order = np.log2(norms[0] / norms[1])
     assert 3.7 < order < 4.3, (norms, order)
+
+
+# ---- point interpolation (Parallel::PatList_Interp_Points) -------------------
+
+import interp as OI
+
+BETA = [18, 19, 20]
+BETA_SOA = [(-1, 1, 1), (1, -1, 1), (1, 1, -1)]
+
+
+def test_interp_points_match_oracle():
+    """Every level of the 3-level hierarchy after a coarse step: the shift
+    (with its parities) and chi at seeded points, bit-identical to the
+    oracle; points outside every patch of a level are not found there."""
+    H = small_hierarchy()
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=1e-6)
+    e = amss_b200.Engine.from_hierarchy(H, precision="fp64", eps=0.1)
+    for i, st in enumerate(init):
+        e.set_state(i, st)
+    e.coarse_step(0.25 * H.h0)
+    assert e.sync() == 0
+    states = [e.get_state(i) for i in range(len(H.blocks))]
+    rng = np.random.default_rng(11)
+    fields = BETA + [0]
+    soa = BETA_SOA + [(1, 1, 1)]
+    for lv in range(len(H.levels)):
+        pb = [H.phys_bbox(p) for p in H.levels[lv]]
+        lo = np.min([b[:3] for b in pb], axis=0)
+        hi = np.max([b[3:] for b in pb], axis=0)
+        pts = rng.uniform(lo - 0.1 * (hi - lo), hi + 0.1 * (hi - lo), size=(40, 3))
+        pts[0] = (1.2, 0.3, -0.4)
+        got, found = e.interp_points(lv, pts, fields, soa)
+        ref, rfound = OI.interp_points(OI.hierarchy_patches(H, lv, states), [tuple(p) for p in pts], fields, soa)
+        assert list(found) == list(rfound)
+        assert found.any() and not found.all()
+        assert np.array_equal(got, np.array(ref))
+    e.close()
+
+
+def test_interp_points_symmetry_plane():
+    """Symmetry 1, blocks added by bbox from the z = 0 plane: points within
+    two cells of the plane interpolate through mirrored cells (betaz odd)."""
+    n, h, lo = 24, 0.25, -3.0
+    hi = lo + n * h
+    mid = lo + 12 * h
+    pbox = (lo, lo, 0.0, hi, hi, n * h)
+    boxes = [(lo, lo, 0.0, mid + 3 * h, hi, n * h), (mid - 3 * h, lo, 0.0, hi, hi, n * h)]
+    e = amss_b200.Engine(precision="fp64", eps=0.1, symmetry=1)
+    for bb in boxes:
+        e.add_block(0, (15, n, n), bb, pbox)
+    e.commit()
+    rng = np.random.default_rng(2)
+    Y = lo + (np.arange(n) + 0.5) * h
+    Z = (np.arange(n) + 0.5) * h
+    blocks = []
+    for bid, bb in enumerate(boxes):
+        X = bb[0] + (np.arange(15) + 0.5) * h
+        st = amss_b200.dropin.get_lousto_nbhs(X, Y, Z, [1.0], [[0.3, -0.2, 0.1]])
+        st += 1e-3 * rng.uniform(-1, 1, st.shape)
+        e.set_state(bid, st)
+        blocks.append((bb, X, Y, Z, st))
+    pts = np.column_stack([rng.uniform(lo, hi, 30), rng.uniform(lo, hi, 30), rng.uniform(0.0, 0.6, 30)])
+    got, found = e.interp_points(0, pts, BETA, BETA_SOA)
+    e.close()
+    patches = [(pbox, [n, n, n], 0, blocks)]
+    ref, rfound = OI.interp_points(patches, [tuple(p) for p in pts], BETA, BETA_SOA, symmetry=1)
+    assert found.all() and all(rfound)
+    assert np.array_equal(got, np.array(ref))
+
+
+# ---- puncture tracking (bssn_class::Step, MAPBH 0) ---------------------------
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_puncture_tracking_matches_oracle(graph):
+    """A shift offset moves the puncture; after 2 coarse steps (8 steps of the
+    finest level) the engine's tracked position equals the oracle's, bit for
+    bit, eager or replayed from a CUDA graph."""
+    H = small_hierarchy()
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=1e-6)
+    for st in init:
+        st[18] += 0.05
+        st[19] -= 0.03
+        st[20] += 0.02
+    dt0 = 0.25 * H.h0
+    start = [[1.2, 0.3, -0.4]]
+    oh = OA.OracleHierarchy(H, eps=0.1)
+    for i, st in enumerate(init):
+        oh.set_state(i, st)
+    oh.set_punctures(start)
+    for _ in range(2):
+        assert oh.coarse_step(dt0) == 0
+    e = amss_b200.Engine.from_hierarchy(H, precision="fp64", eps=0.1)
+    for i, st in enumerate(init):
+        e.set_state(i, st)
+    e.set_punctures(start)
+    if graph:
+        e.run_coarse_graph(dt0, nsteps=1, replays=2)
+    else:
+        for _ in range(2):
+            e.coarse_step(dt0)
+    assert e.sync() == 0
+    got = e.punctures()
+    e.close()
+    ref = np.array(oh.porg0)
+    assert np.array_equal(got, ref), (got, ref)
+    assert abs(got[0, 0] - 1.2) > 5e-3   # it moved, against the shift
+
+
+def test_puncture_tracking_mixed():
+    """The mixed form tracks from its FP32 stages: within 1e-9 of the FP64
+    oracle after 2 coarse steps (the puncture moves by about 1e-2)."""
+    H = small_hierarchy()
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=1e-6)
+    for st in init:
+        st[18] += 0.05
+        st[19] -= 0.03
+        st[20] += 0.02
+    dt0 = 0.25 * H.h0
+    oh = OA.OracleHierarchy(H, eps=0.1)
+    for i, st in enumerate(init):
+        oh.set_state(i, st)
+    oh.set_punctures([[1.2, 0.3, -0.4]])
+    for _ in range(2):
+        assert oh.coarse_step(dt0) == 0
+    e = amss_b200.Engine.from_hierarchy(H, precision="mixed", eps=0.1)
+    for i, st in enumerate(init):
+        e.set_state(i, st)
+    e.set_punctures([[1.2, 0.3, -0.4]])
+    e.run_coarse_graph(dt0, nsteps=1, replays=2)
+    assert e.sync() == 0
+    got = e.punctures()
+    e.close()
+    assert np.abs(got - np.array(oh.porg0)).max() <= 1e-9
