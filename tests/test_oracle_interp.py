@@ -77,3 +77,25 @@ def test_search_walks_down_the_levels():
             assert lev == 0
         else:
             assert lev == len(H.levels) - 1
+
+
+def test_oracle_tracking_follows_a_uniform_shift():
+    """Brill-Lindquist data plus a uniform shift: over one coarse step (4
+    steps of the finest level) the oracle's tracked puncture moves by minus
+    the shift times the elapsed time (RK4 is exact for a constant right-hand
+    side; the shift itself barely changes in that time)."""
+    import amr as OA
+    H = box_in_box(40, 10.0, [(1.2, 0.3, -0.4)], 3, box_cells=32, seed=4, block_min=14, block_max=28)
+    init = OA.initial_state(H, [1.0], [[1.2, 0.3, -0.4]], noise=0.0)
+    beta = (0.05, -0.03, 0.02)
+    for st in init:
+        for v in range(3):
+            st[18 + v] += beta[v]
+    oh = OA.OracleHierarchy(H, eps=0.1)
+    for i, st in enumerate(init):
+        oh.set_state(i, st)
+    oh.set_punctures([[1.2, 0.3, -0.4]])
+    dt0 = 0.25 * H.h0
+    assert oh.coarse_step(dt0) == 0
+    moved = np.array(oh.porg0[0]) - np.array([1.2, 0.3, -0.4])
+    assert np.abs(moved + dt0 * np.array(beta)).max() < 1e-5 * dt0
