@@ -226,7 +226,10 @@ def run_ours(args, rank, world):
         ev1.synchronize()
     nan = eng.sync()
     torch.cuda.synchronize()
-    tracked = eng.punctures().tolist()   # fails if a puncture left the finest level
+    try:
+        tracked = eng.punctures().tolist()
+    except amss_b200.AmssError as exc:   # a puncture left the finest level
+        tracked = str(exc)
     ms = ev0.elapsed_time(ev1)
     launches = eng.launches - launches0
     ms = max_over_ranks(ms, world)
