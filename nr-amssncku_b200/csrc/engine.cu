@@ -1128,7 +1128,7 @@ extern "C" int amss_engine_set_punctures(amss_engine* e, int n, const double* po
   std::memset(&S, 0, sizeof S);
   for (int i = 0; i < 3 * n; ++i) {
     if (!std::isfinite(pos[i])) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_punctures: a position is not finite");
-    S.p0[i] = S.p[i] = pos[i];
+    S.p0[i] = pos[i];
   }
   AMSS_CK(cudaMemcpyAsync(e->dtpatch, tp.data(), tp.size() * sizeof(TrackPatch), cudaMemcpyHostToDevice, e->stream));
   AMSS_CK(cudaMemcpyAsync(e->dtblock, tb.data(), tb.size() * sizeof(TrackBlock), cudaMemcpyHostToDevice, e->stream));

@@ -100,20 +100,22 @@ __global__ void __launch_bounds__(64) k_interp_points(const InterpItem* __restri
 // end): the right-hand side of each coordinate is minus the shift of the
 // substep's input state at the current estimate (compute_Porg_rhs,
 // bssn_class.C:6879-6932), advanced by rungekutta4_scalar
-// (rungekutta4_rout.f90:6-47).  One warp; thread 3p+v owns coordinate v of
-// puncture p.
-__global__ void __launch_bounds__(32) k_track(const TrackPatch* __restrict__ patches, int npatch,
-                                              const TrackBlock* __restrict__ blocks, const int* __restrict__ lvl,
-                                              TrackState* S, int n, int sub, double dt, int symmetry) {
-  const int t = threadIdx.x, p = t / 3, v = t % 3;
-  const bool act = t < 3 * n;
-  double pos[3] = {0.0, 0.0, 0.0};
-  if (act) {
-    const double* src = sub == 0 ? S->p0 : S->p;
-    for (int d = 0; d < 3; ++d) pos[d] = src[3 * p + d];
-  }
-  __syncwarp();
-  if (!act) return;
+// (rungekutta4_rout.f90:6-47).  One CTA per coordinate v of puncture p:
+// every thread repeats the (cheap) search, 36 threads run the z passes of
+// polin3, 6 the y passes, one the x pass and the update.  Substep k reads the
+// estimate of substep k-1 from one buffer and writes the other, so no CTA
+// overwrites a coordinate another CTA still reads.
+constexpr int kTrackThreads = 64;
+
+__global__ void __launch_bounds__(kTrackThreads) k_track(const TrackPatch* __restrict__ patches, int npatch,
+                                                         const TrackBlock* __restrict__ blocks,
+                                                         const int* __restrict__ lvl, TrackState* S, int sub,
+                                                         double dt, int symmetry) {
+  const int p = blockIdx.x / 3, v = blockIdx.x % 3, t = threadIdx.x;
+  // estimate in: Porg0 (substep 0), else the previous substep's
+  const double* src = sub == 0 ? S->p0 : (sub == 2 ? S->pb : S->pa);
+  double pos[3];
+  for (int d = 0; d < 3; ++d) pos[d] = src[3 * p + d];
   int blk = -1;
   const bool finite = isfinite(pos[0]) && isfinite(pos[1]) && isfinite(pos[2]);
   for (int q = 0; q < npatch && blk < 0 && finite; ++q) {
@@ -130,13 +132,13 @@ __global__ void __launch_bounds__(32) k_track(const TrackPatch* __restrict__ pat
     }
     if (blk < 0) break;   // in the patch but in none of its blocks
   }
-  double R = 0.0;
-  if (blk < 0) {
-    atomicOr(&S->err, 1);
-  } else {
+  __shared__ double yat[kOrdn][kOrdn], ym[kOrdn];
+  int cxB[3];
+  double cx[3], soa[3];
+  const void* f = nullptr;
+  bool f32 = false;
+  if (blk >= 0) {
     const TrackBlock& B = blocks[blk];
-    int cxB[3];
-    double cx[3], soa[3];
     for (int d = 0; d < 3; ++d) {
       const double dd = B.dd[d];
       const int cxI = (int)((pos[d] - B.x0[d]) / dd + 0.4) + 1;
@@ -151,13 +153,43 @@ __global__ void __launch_bounds__(32) k_track(const TrackPatch* __restrict__ pat
       soa[d] = d == v ? -1.0 : 1.0;   // beta^v is odd along axis v
     }
     const long long off = (long long)(F_BETAX + v) * B.fs;
-    if (sub == 0)
-      R = -interp_cube(B.tl[lvl[0]] + off, B.ex, cxB, cx, soa);
-    else if (B.f32)   // the mixed form's stages hold the shift in FP32
-      R = -interp_cube((const float*)B.stage[sub == 2 ? 1 : 0] + off, B.ex, cxB, cx, soa);
-    else
-      R = -interp_cube((const double*)B.stage[sub == 2 ? 1 : 0] + off, B.ex, cxB, cx, soa);
+    if (sub == 0) {
+      f = B.tl[lvl[0]] + off;
+    } else if (B.f32) {   // the mixed form's stages hold the shift in FP32
+      f = (const float*)B.stage[sub == 2 ? 1 : 0] + off;
+      f32 = true;
+    } else {
+      f = (const double*)B.stage[sub == 2 ? 1 : 0] + off;
+    }
+    if (t < kOrdn * kOrdn) {   // polin3's z pass for column (a, b)
+      const int a = t / kOrdn, b = t % kOrdn;
+      const int i = cxB[0] + a, j = cxB[1] + b;
+      const long long oi = (i > 0 ? i : 1 - i) - 1, oj = (j > 0 ? j : 1 - j) - 1;
+      const long long sy = B.ex[0], sz = (long long)B.ex[0] * B.ex[1];
+      double yq[kOrdn];
+#pragma unroll
+      for (int c = 0; c < kOrdn; ++c) {
+        const int k = cxB[2] + c;
+        const long long ok = (k > 0 ? k : 1 - k) - 1;
+        const long long o = oi + oj * sy + ok * sz;
+        double val = f32 ? (double)((const float*)f)[o] : ((const double*)f)[o];
+        if (i <= 0) val = val * soa[0];
+        if (j <= 0) val = val * soa[1];
+        if (k <= 0) val = val * soa[2];
+        yq[c] = val;
+      }
+      yat[a][b] = neville6(yq, cx[2]);
+    }
   }
+  __syncthreads();
+  if (blk >= 0 && t < kOrdn) ym[t] = neville6(yat[t], cx[1]);
+  __syncthreads();
+  if (t != 0) return;
+  double R = 0.0;
+  if (blk < 0)
+    atomicOr(&S->err, 1);
+  else
+    R = -neville6(ym, cx[0]);
   const int i = 3 * p + v;
   const double p0 = S->p0[i];
   double pn;
@@ -174,13 +206,16 @@ __global__ void __launch_bounds__(32) k_track(const TrackPatch* __restrict__ pat
     pn = __dadd_rn(p0, __dmul_rn(__dmul_rn(1.0 / 6.0, dt), __dadd_rn(R, S->k[i])));
   }
   if ((symmetry > 0 && v == 2) || (symmetry == 2 && v < 2)) pn = fabs(pn);
-  S->p[i] = pn;
-  if (sub == 3) S->p0[i] = pn;
+  // estimate out: substeps 0 and 2 write pa, substep 1 pb, substep 3 Porg0
+  if (sub == 3)
+    S->p0[i] = pn;
+  else
+    (sub == 1 ? S->pb : S->pa)[i] = pn;
 }
 
 cudaError_t launch_track(const TrackPatch* patches, int npatch, const TrackBlock* blocks, const int* lvl,
                          TrackState* S, int n, int sub, double dt, int symmetry, cudaStream_t s) {
-  k_track<<<1, 32, 0, s>>>(patches, npatch, blocks, lvl, S, n, sub, dt, symmetry);
+  k_track<<<3 * n, kTrackThreads, 0, s>>>(patches, npatch, blocks, lvl, S, sub, dt, symmetry);
   return cudaGetLastError();
 }
 

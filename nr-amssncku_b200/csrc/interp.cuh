@@ -34,10 +34,11 @@ struct TrackBlock {
   int ex[3], cmin[3], f32;
   double flo[3], fhi[3], blo[3], bh[3], x0[3], dd[3];
 };
-constexpr int kMaxPunctures = 10;   // one warp, 3 threads each
+constexpr int kMaxPunctures = 10;
 struct TrackState {
   double p0[3 * kMaxPunctures];     // Porg0: positions at the start of the step
-  double p[3 * kMaxPunctures];      // Porg: the current substep's estimate
+  double pa[3 * kMaxPunctures];     // Porg: the estimates of substeps 0 and 2 ...
+  double pb[3 * kMaxPunctures];     // ... and of substep 1
   double k[3 * kMaxPunctures];      // Porg_rhs: the RK4 accumulator
   int err;                          // a puncture left the finest level
 };
