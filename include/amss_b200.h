@@ -108,8 +108,14 @@ int compute_rhs_z4c_(
  * rule, but no cudaMalloc/cudaFree and no stream creation.  Its device staging
  * area is a static array of the library (23.4 MB per device) that every call
  * shares, so blocks are limited to AMSS_NOALLOC_MAX_POINTS points (and 4096
- * per extent; larger ones fail with AMSS_ERR_ARG), and calls that overlap on
- * the GPU race: serialise them.  Runs on the per-thread default stream. */
+ * per extent; larger ones fail with AMSS_ERR_ARG), and calls that overlapped
+ * on the GPU would race on it: the library serialises the calls of one
+ * process with a lock held until each call's results are on the host.  Runs
+ * on the per-thread default stream.  The first call on a device looks up the
+ * array's address (again after a device reset) and, under CUDA's default lazy
+ * module loading, loads the library's device code, which is when the array's
+ * memory is taken: make that first call before reserving the rest of the
+ * device's memory, and outside any stream capture. */
 #define AMSS_NOALLOC_MAX_POINTS 32768
 int amss_compute_rhs_bssn_noalloc(
     int* ex, double* T, double* X, double* Y, double* Z,

@@ -19,12 +19,23 @@
 //     contents.  All inputs are copied in and every output point is written by
 //     the kernel before it is read back, so only the status word must start at
 //     zero; it is cleared on every call.
-//   * calls that overlap on the GPU (two host threads, or two processes
-//     sharing a context) race on the array: callers must serialise them.
-//   * the symbol's device address is looked up once per device with that
-//     device current (cudaGetSymbolAddress); a caller that captures work on a
-//     stream should make one call first so the lookup is not inside its
-//     capture.
+//   * calls that overlapped on the GPU would race on the array.  The library
+//     holds a lock from a call's first copy until its results are back on
+//     the host, so calls from the threads of one process run one after the
+//     other (another process has its own context and its own copy of the
+//     array); a caller must not run the entry point inside a stream capture.
+//   * the symbol's device address is looked up once per device context with
+//     that device current (cudaGetSymbolAddress), on the first call; a caller
+//     that captures work on a stream should make one call first so the lookup
+//     is not inside its capture.  The lookup is keyed by the context's unique
+//     id (cuCtxGetId), so a caller that resets the device and so gets a new
+//     context gets a fresh lookup instead of a stale address.
+//   * CUDA loads the library's device code lazily (CUDA_MODULE_LOADING=LAZY,
+//     the CUDA 12 default): the first call on a device loads the module and
+//     with it allocates this 23.4 MB array.  A host that reserves the rest of
+//     the device's memory up front should make its first call before that.
+#include <cuda.h>
+
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -57,20 +68,49 @@ constexpr int kMaxDevices = 64;
 std::mutex g_sym_mu;
 double* g_sym_scratch[kMaxDevices] = {};
 unsigned* g_sym_status[kMaxDevices] = {};
+unsigned long long g_sym_ctx[kMaxDevices] = {};   // id of the context the addresses belong to
 
-// Device addresses of the scratch array and status word on the current device.
+// Unique id of the current context (never reused within the process), through
+// the driver entry points the runtime hands out; 0 if unavailable.
+unsigned long long current_ctx_id() {
+  using GetCur = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCur get_cur = nullptr;
+  static GetId get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = (GetCur)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)f;
+  }
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_cur && get_id && get_cur(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+  return 0;
+}
+
+// Device addresses of the scratch array and status word on the current device,
+// looked up once per device context (callers hold g_sym_mu).
 int noalloc_symbols(double** scratch, unsigned** status) {
   int dev = -1;
   AMSS_CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return amss_fail(AMSS_ERR_ARG, "amss_compute_rhs_bssn_noalloc: device index out of range");
-  std::lock_guard<std::mutex> lk(g_sym_mu);
-  if (!g_sym_scratch[dev]) {
+  const unsigned long long ctx = current_ctx_id();   // 0 before the runtime made the context current
+  if (!g_sym_scratch[dev] || ctx == 0 || ctx != g_sym_ctx[dev]) {
     void* a = nullptr;
     void* b = nullptr;
     AMSS_CK(cudaGetSymbolAddress(&a, g_noalloc_scratch));
     AMSS_CK(cudaGetSymbolAddress(&b, g_noalloc_status));
     g_sym_scratch[dev] = (double*)a;
     g_sym_status[dev] = (unsigned*)b;
+    g_sym_ctx[dev] = current_ctx_id();
   }
   *scratch = g_sym_scratch[dev];
   *status = g_sym_status[dev];
@@ -113,6 +153,7 @@ extern "C" int amss_compute_rhs_bssn_noalloc(
   if (check_device("amss_compute_rhs_bssn_noalloc") != 0) return AMSS_ERR_NO_DEVICE;
   double* d = nullptr;
   unsigned* dstatus = nullptr;
+  std::lock_guard<std::mutex> lk(g_sym_mu);
   if (int rc = noalloc_symbols(&d, &dstatus)) return rc;
 
   const long long fs = pad_stride(n);   // <= kNoallocMaxPoints: the limit is a multiple of 64

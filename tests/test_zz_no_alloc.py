@@ -39,3 +39,27 @@ def test_noalloc_matches_allocating_entry_twice():
         assert ref[0] == got[0] == 0
         for r, g in zip(ref[1:], got[1:]):
             assert np.array_equal(r, g)
+
+
+@pytest.mark.gpu
+def test_noalloc_against_oracle_symmetry_and_matter():
+    """Against the oracle (<= 1e-12 relative per output field): a block whose
+    low z face sits on the equatorial plane (Symmetry 1, mirrored pads) with
+    non-zero matter sources, then a block with no symmetry; two calls in a
+    row through the shared static array."""
+    import amss_b200
+    from helpers import relerr
+    rng = np.random.default_rng(17)
+    X = O.cell_coords(-1.5, 1.5, 16)
+    Z = O.cell_coords(0.0, 1.5, 12)
+    st = generic_state(X, X, Z, seed=9)
+    matter = 1e-3 * rng.standard_normal((10, 12, 16, 16))
+    X2, st2 = _block(18, 4)
+    cases = [(X, X, Z, st, matter, 1), (X2, X2, X2, st2, None, 0)]
+    for Xc, Yc, Zc, s, m, sym in cases:
+        ref = O.compute_rhs_bssn(Xc, Yc, Zc, s, matter=m, symmetry=sym, eps=0.1, co=0)
+        got = amss_b200.dropin.compute_rhs_bssn_noalloc(Xc, Yc, Zc, s, matter=m, symmetry=sym, eps=0.1, co=0)
+        assert ref[0] == got[0] == 0
+        for r, g in zip(ref[1:], got[1:]):
+            for f in range(r.shape[0]):
+                assert relerr(g[f], r[f]) <= 1e-12, (sym, f)
