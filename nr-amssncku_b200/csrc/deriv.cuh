@@ -102,8 +102,8 @@ struct PlaneFetch {
       off[e] = o;
     }
   }
-  // issue the loads of plane kk (negative: mirrored, past the end: 0)
-  __device__ __forceinline__ void fetch(int kk) {
+  // issue the loads of plane kk (negative: mirrored, past the end: 0) into w
+  __device__ __forceinline__ void fetch_to(int kk, A* w) const {
     int k = kk;
     bool nz = false;
     if (k < 0) { k = -k - 1; nz = zodd; }
@@ -115,16 +115,18 @@ struct PlaneFetch {
         x = (A)__ldg(src + off[e] + k * sz);
         if ((((neg >> e) & 1u) != 0) != nz) x = -x;
       }
-      v[e] = x;
+      w[e] = x;
     }
   }
-  __device__ __forceinline__ void store(A* slot, int np) const {
+  __device__ __forceinline__ void fetch(int kk) { fetch_to(kk, v); }
+  __device__ __forceinline__ void store_from(A* slot, int np, const A* w) const {
 #pragma unroll
     for (int e = 0; e < DPER; ++e) {
       const int t = threadIdx.x + e * DTHREADS;
-      if (t < np) slot[t] = v[e];
+      if (t < np) slot[t] = w[e];
     }
   }
+  __device__ __forceinline__ void store(A* slot, int np) const { store_from(slot, np, v); }
 };
 
 // Upwinded term of one direction (lopsidediff.f90:321-481) over a line f(o),
@@ -192,13 +194,16 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
   auto dx2 = [&](const A* q) { return C.d2[0] * (-q[-1] + q[1]); };
   auto dy2 = [&](const A* q) { return C.d2[1] * (-q[-DSX] + q[DSX]); };
 
-  // prologue: planes -3 .. 3 one at a time; the column gets -3 .. 3 and the
-  // derivative windows planes -2 .. 1
-#pragma unroll 1
+  // prologue: the loads of planes -3 .. 3 are issued together, then the planes
+  // enter the ring one at a time; the column gets -3 .. 3 and the derivative
+  // windows planes -2 .. 1
+  A pro[7][DPER];
+#pragma unroll
+  for (int m = -3; m <= 3; ++m) P.fetch_to(m, pro[m + 3]);
+#pragma unroll
   for (int m = -3; m <= 3; ++m) {
-    P.fetch(m);
     A* slot = ring + ring_slot(m) * DPLANE;
-    P.store(slot, np);
+    P.store_from(slot, np, pro[m + 3]);
     __syncthreads();
     const A* q = slot + own;
     const A cm = q[0];

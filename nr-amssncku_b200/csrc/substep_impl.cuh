@@ -49,15 +49,19 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
         // the tile's points only (the last tile of a block is short), rounded up to
         // 16 bytes: still inside the block's field, whose stride is a multiple of 64
         const long long nel = N.npts - q0 < 128 ? N.npts - q0 : 128;
-        auto len = [&](int es) { return (unsigned)((nel * es + 15) / 16 * 16); };
         for (int r = threadIdx.x; r < D_SLOTS + 72; r += 32) {
-          const void* a;
-          unsigned bytes;
-          if (r < D_SLOTS) { a = D + N.doff + r * dfs + q0; bytes = len(sizeof(T)); }
-          else if (r < D_SLOTS + 24) { a = nin + (r - D_SLOTS) * fs + q0; bytes = len(sizeof(SI)); }
-          else if (r < D_SLOTS + 48) { a = N.tl[cur] + (r - D_SLOTS - 24) * fs + q0; bytes = len(sizeof(double)); }
-          else { a = N.K + (r - D_SLOTS - 48) * fs + q0; bytes = len(sizeof(double)); }
-          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+          const char* a;
+          int es;
+          if (r < D_SLOTS) { a = (const char*)(D + N.doff + r * dfs + q0); es = sizeof(T); }
+          else if (r < D_SLOTS + 24) { a = (const char*)(nin + (r - D_SLOTS) * fs + q0); es = sizeof(SI); }
+          else if (r < D_SLOTS + 48) { a = (const char*)(N.tl[cur] + (r - D_SLOTS - 24) * fs + q0); es = 8; }
+          else { a = (const char*)(N.K + (r - D_SLOTS - 48) * fs + q0); es = 8; }
+          // the bulk prefetch wants a 16-byte aligned start and a multiple of 16
+          // bytes: the row widened to 16-byte boundaries stays inside the field
+          // row (its base is 256-byte aligned, its stride a multiple of 64)
+          const size_t s0 = (size_t)a & ~(size_t)15;
+          const size_t e0 = ((size_t)a + (size_t)nel * es + 15) & ~(size_t)15;
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s0), "r"((unsigned)(e0 - s0)) : "memory");
         }
       }
      }
