@@ -46,8 +46,7 @@ __global__ void k_amr_sync(const AmrBlock* __restrict__ blocks, const AmrBox* __
       SS* d = (SS*)D.st[sl];
       for (int f = 0; f < D.nf; ++f) d[f * D.fs + od] = s[f * S.fs + os];
       if constexpr (sizeof(SS) == 4) {
-        D.side[sl][od] = S.side[sl][os];
-        D.side[sl][D.fs + od] = S.side[sl][S.fs + os];
+        for (int f = 0; f < kSideFields; ++f) D.side[sl][f * D.fs + od] = S.side[sl][f * S.fs + os];
       }
     }
   }

@@ -11,7 +11,7 @@ struct AmrBlock {
   long long fs;
   double* tl[3];       // three time levels of the FP64 state; tl[cur] is current
   void* st[2];         // stage buffers (FP64, or FP32 in the mixed form)
-  double* side[2];     // FP64 chi, alpha of the stages (mixed form)
+  double* side[2];     // FP64 chi, alpha, beta^i of the stages (mixed form, kSideFields each)
   double* K;           // RK accumulator, reused as the time-interpolated parent state
   const int* lvl;      // level state {cur, steps taken}
   int nf;              // evolved fields: 24 (BSSN) or 25 (Z4c)

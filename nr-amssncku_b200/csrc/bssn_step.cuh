@@ -73,7 +73,7 @@ struct EpiRK {
   const double* u0;   // state at t_n (FP64)
   double* K;          // RK accumulator (FP64)
   SO* out;            // stage output, or the new state at sub == 3
-  double* out_side;   // FP64 chi, alpha of an FP32 stage output
+  double* out_side;   // FP64 side slots (chi, alpha, beta^i) of an FP32 stage output
   long long fs, p;
   int sub;
   bool freeze;        // outer face of a refined patch: output = u0 there
@@ -169,7 +169,7 @@ struct StepBlock {
                       // tl[(cur+1)%3] receives U_new (it held t_n - 2 dt)
   const int* lvl;     // level state {cur, steps taken} (device, rotated after each step)
   void* stage[2];     // stage buffers A and B (type of the stage storage)
-  double* side[2];    // FP64 chi, alpha of stages A and B (mixed form only)
+  double* side[2];    // FP64 side slots (chi, alpha, beta^i) of stages A and B (mixed form only)
   double* K;          // RK accumulator (FP64)
   long long doff;     // offset of this block's points in the level's D slots (split form)
   long long npts;

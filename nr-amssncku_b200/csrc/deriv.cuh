@@ -50,13 +50,8 @@ constexpr bool deriv_planes_fit(int w) {
 }
 static_assert(deriv_planes_fit(kDerivMinEx), "plane buffer too small for a tile shape");
 
-// points per tile (= threads per CTA) of the staged pointwise pass (substep_staged.cuh)
-constexpr int STILE = 64;
-#ifndef AMSS_POINTWISE_STAGED   // pointwise pass of the split form: 1 staged in shared memory, 0 per-thread loads
-#define AMSS_POINTWISE_STAGED 0
-#endif
 // substep tile of the split form's pointwise pass
-constexpr int kPointwiseTile = AMSS_POINTWISE_STAGED ? STILE : 128;
+constexpr int kPointwiseTile = 128;
 
 struct DerivItem {
   int block;   // index into the level's StepBlock table
@@ -161,8 +156,8 @@ __device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, i
 // field's source array, SI: type of the stage input (for the shift), T: type
 // of the D array.
 template <typename A, int KIND, typename T, typename S, typename SI>
-__device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, int F, int x0,
-                                             int y0, T* D, long long dfs, A* ring) {
+__device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, const double* bsh,
+                                             int F, int x0, int y0, T* D, long long dfs, A* ring) {
   const Coef<A>& C = pick<A>(B.C);
   const int ex0 = B.b.ex[0], ex1 = B.b.ex[1], ex2 = B.b.ex[2];
   const long long fs = B.b.fs;
@@ -305,10 +300,12 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
       }
       A adv = A(0);
       if (G.lop) {
-        // the shift at the point, from the stage input (never a wide field)
-        const T bx = (T)__ldg(in + F_BETAX * fs + p);
-        const T by = (T)__ldg(in + F_BETAY * fs + p);
-        const T bz = (T)__ldg(in + F_BETAZ * fs + p);
+        // the shift at the point, from the stage input (bsh: its FP64 side
+        // slots in the mixed form), rounded to the storage type T of the
+        // other fields as the pointwise pass sees it
+        const T bx = bsh ? (T)__ldg(bsh + p) : (T)__ldg(in + F_BETAX * fs + p);
+        const T by = bsh ? (T)__ldg(bsh + fs + p) : (T)__ldg(in + F_BETAY * fs + p);
+        const T bz = bsh ? (T)__ldg(bsh + 2 * fs + p) : (T)__ldg(in + F_BETAZ * fs + p);
         auto Xp = [&](int dd) { return X(dd) + add1; };
         auto Yp = [&](int dd) { return Y(dd) + add1; };
         auto Zp = [&](int dd) { return Z(dd) + add1; };
@@ -359,21 +356,23 @@ __global__ void __launch_bounds__(DTHREADS, 2) k_deriv(const StepBlock<T>* __res
     const SI* in = sub == 0 ? (const SI*)B.tl[cur] : (const SI*)B.stage[sub == 2 ? 1 : 0];
     const int F = it.field;
     const long long fs = B.b.fs;
+    // the mixed form's stages keep the shift in their FP64 side slots
+    const double* bsh = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F_BETAX) * fs : nullptr;
     if constexpr (sizeof(T) == 4) {
-      if (F == F_CHI || F == F_LAP) {
+      if (is_wide(F)) {
         // wide fields of the mixed form: FP64 source (state, or the FP64 side stage) and arithmetic
         const double* src = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F) * fs
                                             : (const double*)in + F * fs;
-        deriv_column<double, 0>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<double*>(smem));
+        deriv_column<double, 0>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<double*>(smem));
         __syncthreads();
         continue;
       }
     }
     const SI* src = in + F * fs;
     switch (dkind(F)) {
-      case 0: deriv_column<T, 0>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
-      case 1: deriv_column<T, 1>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
-      default: deriv_column<T, 2>(B, src, in, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      default: deriv_column<T, 2>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
     }
     __syncthreads();
   }

@@ -577,7 +577,7 @@ extern "C" int amss_engine_commit(amss_engine* e) {
     bytes += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
     bytes += align((size_t)e->nf * b.fs * sizeof(double)) * 4;  // 3 time levels + K
     bytes += align((size_t)e->nf * b.fs * ss) * 2;              // two stages
-    if (mixed) bytes += align((size_t)2 * b.fs * sizeof(double)) * 2;
+    if (mixed) bytes += align((size_t)kSideFields * b.fs * sizeof(double)) * 2;
   }
   AMSS_CK(cudaMalloc(&e->arena, bytes));
   AMSS_CK(cudaMemset(e->arena, 0, bytes));
@@ -591,8 +591,8 @@ extern "C" int amss_engine_commit(amss_engine* e) {
     b.st[0] = p; p += align((size_t)e->nf * b.fs * ss);
     b.st[1] = p; p += align((size_t)e->nf * b.fs * ss);
     if (mixed) {
-      b.side[0] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
-      b.side[1] = (double*)p; p += align((size_t)2 * b.fs * sizeof(double));
+      b.side[0] = (double*)p; p += align((size_t)kSideFields * b.fs * sizeof(double));
+      b.side[1] = (double*)p; p += align((size_t)kSideFields * b.fs * sizeof(double));
     }
     AMSS_CK(cudaMemcpy(b.dX, b.X.data(), b.ex[0] * sizeof(double), cudaMemcpyHostToDevice));
     AMSS_CK(cudaMemcpy(b.dX + b.ex[0], b.Y.data(), b.ex[1] * sizeof(double), cudaMemcpyHostToDevice));
@@ -1099,6 +1099,8 @@ extern "C" int amss_engine_set_punctures(amss_engine* e, int n, const double* po
       for (int t = 0; t < 3; ++t) B.tl[t] = b.tl[t];
       B.stage[0] = b.st[0];
       B.stage[1] = b.st[1];
+      B.side[0] = b.side[0];
+      B.side[1] = b.side[1];
       B.f32 = e->prm.precision == 1;
       B.fs = b.fs;
       find_box(b, q, B.flo, B.fhi);

@@ -135,8 +135,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_track(const TrackPatch* __res
   __shared__ double yat[kOrdn][kOrdn], ym[kOrdn];
   int cxB[3];
   double cx[3], soa[3];
-  const void* f = nullptr;
-  bool f32 = false;
+  const double* f = nullptr;
   if (blk >= 0) {
     const TrackBlock& B = blocks[blk];
     for (int d = 0; d < 3; ++d) {
@@ -155,9 +154,8 @@ __global__ void __launch_bounds__(kTrackThreads) k_track(const TrackPatch* __res
     const long long off = (long long)(F_BETAX + v) * B.fs;
     if (sub == 0) {
       f = B.tl[lvl[0]] + off;
-    } else if (B.f32) {   // the mixed form's stages hold the shift in FP32
-      f = (const float*)B.stage[sub == 2 ? 1 : 0] + off;
-      f32 = true;
+    } else if (B.f32) {   // the mixed form's stages hold the shift in their FP64 side slots
+      f = B.side[sub == 2 ? 1 : 0] + (long long)(kSideBetaX + v) * B.fs;
     } else {
       f = (const double*)B.stage[sub == 2 ? 1 : 0] + off;
     }
@@ -172,7 +170,7 @@ __global__ void __launch_bounds__(kTrackThreads) k_track(const TrackPatch* __res
         const int k = cxB[2] + c;
         const long long ok = (k > 0 ? k : 1 - k) - 1;
         const long long o = oi + oj * sy + ok * sz;
-        double val = f32 ? (double)((const float*)f)[o] : ((const double*)f)[o];
+        double val = f[o];
         if (i <= 0) val = val * soa[0];
         if (j <= 0) val = val * soa[1];
         if (k <= 0) val = val * soa[2];

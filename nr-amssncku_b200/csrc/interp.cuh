@@ -27,9 +27,11 @@ struct TrackPatch {
 // A block: its state arrays (stages FP32 when f32), the box it answers for (Patch::Interp_Points),
 // its cell-centre coordinates X(j) = blo + (j - 0.5) bh, X(1), X(2) - X(1),
 // and the first stencil index allowed (-2 at a symmetry plane).
+constexpr int kSideBetaX = 2;   // side slot of beta^x in the mixed form's FP64 stage fields (stencil.cuh)
 struct TrackBlock {
   const double* tl[3];
   const void* stage[2];
+  const double* side[2];   // FP64 side slots of the stages (mixed form: the shift is read there)
   long long fs;
   int ex[3], cmin[3], f32;
   double flo[3], fhi[3], blo[3], bh[3], x0[3], dd[3];

@@ -29,13 +29,27 @@ struct Coef {
   T ko;              // eps/64
 };
 
-// chi and alpha carry O(1) backgrounds: an FP32 copy of them costs ~6e-8 * |f|
-// absolute, which a second derivative turns into a relative RHS error of
-// ~6e-8 (L/dx)^2.  In the mixed form they therefore keep FP64 stage storage
-// ("side" arrays) and FP64 stencil arithmetic; every other field is FP32.
+// An FP32 copy of a field f costs ~6e-8 |f| absolute, which a second
+// derivative turns into an RHS error of ~6e-8 |f| (4 / dx^2), a stencil's
+// cancellation of the field's own size.  chi and alpha carry O(1)
+// backgrounds; the shift grows to O(0.1 - 1) near the punctures and its
+// second derivatives drive Gamma~^i (gamma~^jk d_j d_k beta^i) and through it
+// B^i.  In the mixed form these five fields therefore keep FP64 stage storage
+// ("side" arrays, slots chi, alpha, beta^x, beta^y, beta^z) and FP64 stencil
+// arithmetic, whose results are rounded only once, relative to the
+// derivative itself; every other field is FP32.
 template <int F>
-__host__ __device__ constexpr bool wide_field() { return F == F_CHI || F == F_LAP; }
-__host__ __device__ constexpr int side_slot(int F) { return F == F_CHI ? 0 : 1; }
+__host__ __device__ constexpr bool wide_field() {
+  return F == F_CHI || F == F_LAP || F == F_BETAX || F == F_BETAY || F == F_BETAZ;
+}
+__host__ __device__ constexpr bool is_wide(int F) {
+  return F == F_CHI || F == F_LAP || F == F_BETAX || F == F_BETAY || F == F_BETAZ;
+}
+__host__ __device__ constexpr int side_slot(int F) {
+  return F == F_CHI ? 0 : (F == F_LAP ? 1 : 2 + (F - F_BETAX));
+}
+constexpr int kSideFields = 5;   // FP64 stage fields of the mixed form
+static_assert(side_slot(F_BETAX) == 2, "interp.cuh reads the shift from side slot 2");
 
 // Coefficients in the arithmetic type and in FP64 (for the wide fields).
 template <typename T>
@@ -58,7 +72,7 @@ struct Pt {
   static constexpr bool kPre = false;
   using elem = SI;
   const SI* __restrict__ base;  // field 0 of the block
-  const double* __restrict__ side;  // FP64 chi, alpha when SI is float (else unused)
+  const double* __restrict__ side;  // FP64 side slots (chi, alpha, beta^i) when SI is float (else unused)
   long long fs;                 // field stride
   long long p;                  // linear index of the point
   long long sy, sz;             // strides of j and k

@@ -2,7 +2,7 @@
 // Instantiated in one translation unit per (precision, symmetry) pair so the
 // large kernels compile in parallel.
 #pragma once
-#include "substep_staged.cuh"
+#include "substep_common.cuh"
 
 #ifndef AMSS_SUBSTEP_MINB   // resident CTAs of 128 threads the register-pass kernel is compiled for
 #define AMSS_SUBSTEP_MINB 2
@@ -153,34 +153,19 @@ cudaError_t launch_face(const void* blocks, const int2* faces, int nfaces, int s
   return cudaGetLastError();
 }
 
-// SPLIT: the pointwise pass -- staged through shared memory over
-// STILE-point tiles when AMSS_POINTWISE_STAGED, else per-thread loads over
-// 128-point tiles (kPointwiseTile); otherwise the fused kernel (128-point tiles).
+// SPLIT: the pointwise pass of the split form (per-thread loads over
+// 128-point tiles); otherwise the fused kernel (128-point tiles).
 template <typename T, typename SS, bool SYMM, bool SPLIT, bool Z4C>
 cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, int sub, RKConst rk, int enforce,
                            unsigned* status, int grid, cudaStream_t s, const void* D, long long dfs) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
   const T* d = (const T*)D;
-  if constexpr (SPLIT && AMSS_POINTWISE_STAGED && !Z4C) {
-#define AMSS_STAGED(SI, SO)                                                                          \
-    {                                                                                                \
-      constexpr size_t sm = staged_smem_bytes<T, SI>();                                              \
-      cudaFuncSetAttribute(k_substep_staged<T, SI, SO, SYMM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                           (int)sm);                                                                 \
-      k_substep_staged<T, SI, SO, SYMM><<<grid, STILE, sm, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs); \
-    }
-    if (sub == 0) AMSS_STAGED(double, SS)
-    else if (sub == 3) AMSS_STAGED(SS, double)
-    else AMSS_STAGED(SS, SS)
-#undef AMSS_STAGED
-  } else {
-    if (sub == 0)
-      k_substep<T, double, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
-    else if (sub == 3)
-      k_substep<T, SS, double, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
-    else
-      k_substep<T, SS, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
-  }
+  if (sub == 0)
+    k_substep<T, double, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  else if (sub == 3)
+    k_substep<T, SS, double, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
+  else
+    k_substep<T, SS, SS, SYMM, SPLIT, Z4C><<<grid, 128, 0, s>>>(bl, tiles, ntiles, sub, rk, enforce, status, d, dfs);
   return cudaGetLastError();
 }
 
