@@ -37,10 +37,14 @@ sys.path.insert(0, os.path.join(ROOT, "nr-amssncku_b200"))
 
 METRIC = "BSSN RK4 zone-updates/s on 1 B200: FP64 vs mixed, %HBM peak; adjoint/fwd ratio"
 # algorithmic HBM bytes per zone-update: every field array read or written once per
-# substep, 17 words per field per step.  Mixed: FP32 stages for all but chi and
-# alpha, FP64 stages for those two, FP64 U0/K/U_new: (nf - 2) * 112 + 2 * 136.
+# substep, 17 words per field per step.  Mixed: FP32 stages for all but the five
+# wide fields (chi, alpha, beta^i), FP64 stages for those, FP64 U0/K/U_new:
+# (nf - 5) * 112 + 5 * 136.
+WIDE_FIELDS = 5
+
+
 def bytes_per_zone(precision, nf):
-    return 17 * nf * 8 if precision == "fp64" else (nf - 2) * 112 + 2 * 136
+    return 17 * nf * 8 if precision == "fp64" else (nf - WIDE_FIELDS) * 112 + WIDE_FIELDS * 136
 
 
 def workload(name):
@@ -159,15 +163,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(precision, formulation):
-    """DRAM bytes per point-step of the substep kernels (k_deriv + k_substep)
-    from the committed ncu summary, if one exists for this precision and
-    formulation; same unit as algorithmic_bytes_per_point_step."""
+def ncu_traffic(precision, formulation, workload):
+    """DRAM bytes per interior zone-update of the substep kernels from the
+    committed ncu summary (profiles/substep_traffic.json), with the workload
+    and capture it was taken on; (None, why) when there is none for this
+    precision and formulation."""
     p = os.path.join(ROOT, "profiles", "substep_traffic.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get(precision if formulation == "bssn" else f"z4c_{precision}")
-    return None
+    if not os.path.exists(p):
+        return None, "no ncu summary committed"
+    d = json.load(open(p))
+    key = precision if formulation == "bssn" else f"z4c_{precision}"
+    for entry in d.get("captures", []):
+        if entry.get("key") == key and entry.get("workload") == workload:
+            return entry["bytes_per_zone_update"], entry["source"]
+    for entry in d.get("captures", []):
+        if entry.get("key") == key:
+            return entry["bytes_per_zone_update"], entry["source"] + f" (a {entry['workload']} capture, not {workload})"
+    return None, f"no ncu capture for {key}"
 
 
 def max_over_ranks(value, world, device="cuda"):
@@ -186,30 +198,27 @@ def job_rate(units_per_rank, world, ms_per_step):
     return units_per_rank * world / (ms_per_step * 1e-3)
 
 
-def run_ours(args, rank, world):
+def time_engine(args, w, init, precision, rank, world, dev):
+    """One engine form over the workload: warm-up, K coarse steps replayed as
+    a CUDA graph (CUDA events on the engine's stream, bracketed by a barrier
+    and a synchronize, max over ranks), then the end-to-end steps through the
+    public API with pinned host buffers.  Returns the timings."""
     import torch
     import amss_b200
 
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    w = workload(args.workload)
     H = w["H"]
-    nf = 25 if args.formulation == "z4c" else 24
-    init = make_initial(w, nf)
     dt0 = w["courant"] * H.h0
-    zones, npts = counts(H)
-    eng = amss_b200.Engine.from_hierarchy(H, precision=args.precision, eps=w["eps"], kernel=args.kernel,
+    eng = amss_b200.Engine.from_hierarchy(H, precision=precision, eps=w["eps"], kernel=args.kernel,
                                           formulation=args.formulation)
     for i, st in enumerate(init):
         eng.set_state(i, st)
     eng.set_punctures(w["pos"])   # Step tracks the punctures on the finest level (MAPBH 0)
     stream = torch.cuda.ExternalStream(eng.stream)
 
-    # warm-up, then K timed steps bracketed by a barrier + synchronize
     for _ in range(args.warmup):
         eng.coarse_step(dt0)
     if eng.sync():
-        raise SystemExit("NaN during warm-up")
+        raise SystemExit(f"{precision}: NaN during warm-up")
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -230,12 +239,10 @@ def run_ours(args, rank, world):
         tracked = eng.punctures().tolist()
     except amss_b200.AmssError as exc:   # a puncture left the finest level
         tracked = str(exc)
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     launches = eng.launches - launches0
-    ms = max_over_ranks(ms, world)
     if world > 1:
         torch.distributed.barrier()
-    ms_per_step = ms / args.steps
 
     # end to end through the public API: every block's state in from pinned host
     # memory, one coarse step, every block's state out
@@ -255,15 +262,40 @@ def run_ours(args, rank, world):
         for i, ho in enumerate(host_out):
             eng.get_state(i, out=ho)          # device -> host copy of the step's result
     t1 = time.perf_counter()
-    e2e_ms = (t1 - t0) * 1e3 / e2e_steps
-    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_ms = max_over_ranks((t1 - t0) * 1e3 / e2e_steps, world)
     eng.close()
+    return dict(ms_per_step=ms / args.steps, e2e_ms=e2e_ms, launches=launches, clocks=clk.summary(),
+                nan=bool(nan), tracked=tracked)
+
+
+def roofline(precision, nf, zones, ms_per_step, npts, peak):
+    """HBM roofline of a coarse step: algorithmic bytes per interior
+    zone-update x interior zone-updates / step time.  Array-point bandwidth
+    (ghost and buffer cells counted as work too) is reported beside it."""
+    bpz = bytes_per_zone(precision, nf)
+    achieved = bpz * zones / (ms_per_step * 1e-3) / 1e9
+    return dict(achieved=achieved, frac=achieved / peak, algorithmic_bytes_per_zone_update=bpz,
+                array_point_gbs=bpz * npts / (ms_per_step * 1e-3) / 1e9)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w = workload(args.workload)
+    H = w["H"]
+    nf = 25 if args.formulation == "z4c" else 24
+    init = make_initial(w, nf)
+    zones, npts = counts(H)
+    hbm_peak, peak_kind = peaks()
     state_bytes = int(sum(st.nbytes for st in init))
 
+    r = time_engine(args, w, init, args.precision, rank, world, dev)
+    ms_per_step = r["ms_per_step"]
     value = job_rate(zones, world, ms_per_step)
-    hbm_peak, peak_kind = peaks()
-    bpz = bytes_per_zone(args.precision, nf)
-    achieved = bpz * npts / (ms_per_step * 1e-3) / 1e9
+    rf = roofline(args.precision, nf, zones, ms_per_step, npts, hbm_peak)
+    traffic, traffic_src = ncu_traffic(args.precision, args.formulation, args.workload)
     line = {
         "metric": METRIC,
         "value": value,
@@ -285,21 +317,39 @@ def run_ours(args, rank, world):
                                         "inside the step",
                    "l2": "state + stages + K of the hierarchy (GBs) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{world} (no data-path collective)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": ncu_traffic(args.precision, args.formulation),
-                     "traffic_unit": "B/point-step",
+        "roofline": {"bound": "hbm", "achieved": rf["achieved"], "peak": hbm_peak, "unit": "GB/s",
+                     "frac": rf["frac"], "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_unit": "B/zone-update", "traffic_source": traffic_src,
                      "kernel": "whole coarse step: RK4 substeps (stencil pass + pointwise pass) and the AMR "
                                "transfers, timed together",
-                     "algorithmic_bytes_per_point_step": bpz},
-        "e2e": {"value": job_rate(zones, world, e2e_ms), "unit": "zone-updates/s",
+                     "algorithmic_bytes_per_zone_update": rf["algorithmic_bytes_per_zone_update"],
+                     "achieved_per_array_point_gbs": rf["array_point_gbs"]},
+        "e2e": {"value": job_rate(zones, world, r["e2e_ms"]), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "path": "amss_b200.Engine set_state (pinned, every block) -> coarse_step -> get_state"},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
-        "nan": bool(nan),
-        "punctures_after_warmup_and_timed_steps": tracked,
+        "gpu_launches": int(r["launches"]),
+        "clocks": r["clocks"],
+        "nan": r["nan"],
+        "punctures_after_warmup_and_timed_steps": r["tracked"],
     }
+    if args.precision == "fp64" and args.formulation == "bssn" and not args.no_parts:
+        # the metric's other two parts: the mixed form on the same workload, and
+        # the adjoint/forward step ratio of the 96^3 gradient workload
+        m = time_engine(args, w, init, "mixed", rank, world, dev)
+        mrf = roofline("mixed", nf, zones, m["ms_per_step"], npts, hbm_peak)
+        line["mixed"] = {"value": job_rate(zones, world, m["ms_per_step"]), "unit": "zone-updates/s",
+                         "ms_per_step": m["ms_per_step"],
+                         "e2e": job_rate(zones, world, m["e2e_ms"]), "roofline_frac": mrf["frac"],
+                         "roofline_achieved": mrf["achieved"],
+                         "algorithmic_bytes_per_zone_update": mrf["algorithmic_bytes_per_zone_update"],
+                         "gpu_launches": int(m["launches"]), "clocks": m["clocks"], "nan": m["nan"]}
+        line["mixed_over_fp64"] = ms_per_step / m["ms_per_step"]
+        if world == 1:
+            a = run_adjoint(args, steps=1, warmup=1)
+            line["adjoint"] = {k: a[k] for k in ("metric", "value", "unit", "forward_ms_per_step",
+                                                 "adjoint_ms_per_step", "engine_forward_ms_per_step",
+                                                 "adjoint_vs_engine_step", "gpu_launches", "clocks")}
+            line["adjoint_over_forward"] = a["value"]
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w, init)
     return line
@@ -336,7 +386,7 @@ def cpu_baseline(args, w, init, budget_s=12.0):
                       f"zones), FP64, OpenMP over {cores} threads"}
 
 
-def run_adjoint(args):
+def run_adjoint(args, steps=None, warmup=None):
     """adjoint96: the gradient of L = sum_interior H^2 dV after 200 FP64 RK4
     steps (checkpoint every 20) on one 96^3-interior block on [-12, 12]^3,
     Brill-Lindquist m = 1 at (0.1, 0.05, 0.02) plus a Gaussian on gamma~_xx
@@ -350,6 +400,8 @@ def run_adjoint(args):
     from amss_b200.adjoint import Adjoint
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     n, nsteps, ck = args.adj_n, args.adj_steps, args.adj_ck
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     X, st, bbox, h = initial.single_block_state(n, -n / 8.0, n / 8.0, 3, [1.0], [[0.1, 0.05, 0.02]])
     rng = np.random.default_rng(1)
     while True:
@@ -361,9 +413,9 @@ def run_adjoint(args):
     ex = (len(X),) * 3
     adj = Adjoint(ex, bbox)
     stream = torch.cuda.ExternalStream(adj.stream)
-    for w_i in range(args.warmup):   # the last at full length: checkpoint and segment storage get allocated
+    for w_i in range(warmup):   # the last at full length: checkpoint and segment storage get allocated
         adj.set_state(st)
-        if w_i == args.warmup - 1:
+        if w_i == warmup - 1:
             adj.forward(dt, nsteps, ck)
         else:
             adj.forward(dt, min(nsteps, 2), 1)
@@ -380,7 +432,7 @@ def run_adjoint(args):
 
     fwd, bwd = [], []
     with ClockSampler(torch.cuda.current_device()) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             adj.set_state(st)
             l0 = adj.launches
             t, loss = timed(lambda: adj.forward(dt, nsteps, ck))
@@ -413,7 +465,7 @@ def run_adjoint(args):
     return {
         "metric": f"adjoint step time / forward step time (FP64, {n}^3, {nsteps} RK4 steps, checkpoint every {ck})",
         "value": round(b_ms / f_ms, 3), "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic (Brill-Lindquist + "
+        "steps": steps, "warmup": warmup, "dtype": "f64", "data": "synthetic (Brill-Lindquist + "
         "Gaussian on gamma~_xx, generated in-process)",
         "forward_ms_per_step": round(f_ms, 4), "adjoint_ms_per_step": round(b_ms, 4),
         "engine_forward_ms_per_step": round(eng_ms, 4), "adjoint_vs_engine_step": round(b_ms / eng_ms, 3),
@@ -537,6 +589,8 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parts", action="store_true",
+                    help="FP64 line only: skip the mixed-form and adjoint parts of the metric")
     ap.add_argument("--report", choices=["none", "mixed"], default="none",
                     help="mixed: the mixed form's field and constraint errors against FP64 (amr3 hierarchy)")
     ap.add_argument("--report-steps", type=int, default=20)
@@ -546,6 +600,9 @@ def main():
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.gpus != world:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}: launch N > 1 ranks with torchrun "
+                         f"(python -m torch.distributed.run --nproc-per-node N bench.py --gpus N)")
     if args.report == "mixed":
         if rank == 0:
             print(json.dumps(run_mixed_report(args)))
