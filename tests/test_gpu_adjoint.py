@@ -149,6 +149,36 @@ def test_gradient_matches_finite_differences_full_state():
     adj.close()
 
 
+def test_gradient_with_shift_directions():
+    """Directions that perturb the shift too.  The state carries a smooth
+    shift bounded away from zero (|beta^i| >= 0.02), so a 1e-6 step keeps the
+    upwind side of every advection stencil and the central difference sees
+    no kink; the directions then include beta^i, B^i and every other field."""
+    X, st0, bbox, h = _block(noise=1e-6)
+    z, y, x = np.meshgrid(X, X, X, indexing="ij")
+    st0[18] += 0.05 + 0.02 * np.sin(0.7 * x) * np.cos(0.5 * y)
+    st0[19] += -0.04 + 0.015 * np.cos(0.6 * z)
+    st0[20] += 0.03 + 0.008 * np.sin(0.4 * x + 0.3 * z)
+    assert np.abs(st0[18:21]).min() >= 0.02
+    dt = 0.25 * h
+    nsteps, ck = 6, 4
+    adj = amss_b200.adjoint.Adjoint((len(X),) * 3, bbox)
+    adj.set_state(st0)
+    adj.forward(dt, nsteps, ck)
+    g = adj.backward()
+    assert np.all(np.isfinite(g))
+    rng = np.random.default_rng(13)
+    for trial in range(4):
+        v = rng.standard_normal(st0.shape)
+        v *= np.abs(st0).max(axis=(1, 2, 3), keepdims=True).clip(1e-3, 1.0)
+        v[0] = rng.standard_normal(st0.shape[1:]) * (1.0 + st0[0])
+        v[17] = rng.standard_normal(st0.shape[1:]) * (1.0 + st0[17])
+        an = float(np.sum(g * v))
+        fd = _directional(adj, st0, dt, nsteps, ck, v)
+        assert abs(fd - an) <= 1e-6 * max(abs(fd), abs(an)), (trial, fd, an)
+    adj.close()
+
+
 def test_checkpoint_interval_does_not_change_the_gradient():
     X, st0, bbox, h = _block(n=16, lo=-2.0, hi=2.0)
     dt = 0.25 * h
