@@ -139,46 +139,69 @@ def single_block(n_interior, lo, hi, ghosts=3):
     return H
 
 
+def merge_boxes(boxes, buffer=BUFFER):
+    """Merge the boxes [lo, hi) of one level whose buffered extents meet into
+    their bounding box, until no two meet.  The reference merges boxes that
+    touch or overlap into their bounding box when that box is filled well
+    enough (Parallel::merge_gs, Parallel.C:4997-5086) and cuts the others
+    apart (cut_gsl); patches of this engine may not touch even through their
+    buffers, so any two whose buffered boxes meet are merged."""
+    boxes = [[list(lo), list(hi)] for lo, hi in boxes]
+    merged = True
+    while merged:
+        merged = False
+        for a in range(len(boxes)):
+            for b in range(a + 1, len(boxes)):
+                A, B = boxes[a], boxes[b]
+                if all(A[0][d] - buffer <= B[1][d] + buffer and B[0][d] - buffer <= A[1][d] + buffer
+                       for d in range(3)):
+                    boxes[a] = [[min(A[0][d], B[0][d]) for d in range(3)], [max(A[1][d], B[1][d]) for d in range(3)]]
+                    del boxes[b]
+                    merged = True
+                    break
+            if merged:
+                break
+    return boxes
+
+
+def from_boxes(x0, h0, coarse, levels, seed=1, block_min=24, block_max=80):
+    """A hierarchy with the level-0 patch [0, coarse) (cells per axis) and, for
+    levels 1.., the boxes levels[l - 1] (lists of [lo, hi) in that level's
+    global cells), merged as merge_boxes does; every patch is split into seeded
+    uneven blocks of block_min..block_max cells per side."""
+    rng = np.random.default_rng(seed)
+    coarse = tuple(coarse) if np.ndim(coarse) else (int(coarse),) * 3
+    H = Hierarchy(x0, h0)
+    H.add_patch(0, (0, 0, 0), coarse, 0, [_splits(0, coarse[d], rng, block_min, block_max) for d in range(3)])
+    for lev, boxes in enumerate(levels, start=1):
+        for lo, hi in merge_boxes(boxes):
+            H.add_patch(lev, lo, hi, BUFFER,
+                        [_splits(lo[d] - BUFFER, hi[d] + BUFFER, rng, block_min, block_max) for d in range(3)])
+    H.check_nesting()
+    return H
+
+
 def box_in_box(coarse_cells, extent, centres, nlevels, box_cells=48, seed=1, block_min=24, block_max=80):
     """Config-2 style hierarchy: level 0 covers [-extent, extent]^3 with
     coarse_cells per side; levels 1..nlevels-1 carry one box of box_cells per
     side (in that level's cells) around each centre, boxes whose buffered
     extents overlap merged into their bounding box; every patch is split into
     seeded uneven blocks of block_min..block_max cells per side."""
-    rng = np.random.default_rng(seed)
     h0 = 2.0 * extent / coarse_cells
-    H = Hierarchy(-extent, h0)
-    H.add_patch(0, (0, 0, 0), (coarse_cells,) * 3, 0,
-                [_splits(0, coarse_cells, rng, block_min, block_max) for _ in range(3)])
+    x0 = -extent
+    levels = []
     for lev in range(1, nlevels):
-        h = H.h(lev)
+        h = h0 / 2 ** lev
         boxes = []
         for c in centres:
             lo = []
             for d in range(3):
-                ci = int(round((c[d] - H.x0) / h))
+                ci = int(round((c[d] - x0) / h))
                 l0 = ci - box_cells // 2
                 lo.append(l0 - (l0 % 2))
             boxes.append([lo, [v + box_cells for v in lo]])
-        merged = True
-        while merged:
-            merged = False
-            for a in range(len(boxes)):
-                for b in range(a + 1, len(boxes)):
-                    A, B = boxes[a], boxes[b]
-                    if all(A[0][d] - BUFFER <= B[1][d] + BUFFER and B[0][d] - BUFFER <= A[1][d] + BUFFER
-                           for d in range(3)):
-                        boxes[a] = [[min(A[0][d], B[0][d]) for d in range(3)], [max(A[1][d], B[1][d]) for d in range(3)]]
-                        del boxes[b]
-                        merged = True
-                        break
-                if merged:
-                    break
-        for lo, hi in boxes:
-            H.add_patch(lev, lo, hi, BUFFER,
-                        [_splits(lo[d] - BUFFER, hi[d] + BUFFER, rng, block_min, block_max) for d in range(3)])
-    H.check_nesting()
-    return H
+        levels.append(boxes)
+    return from_boxes(x0, h0, coarse_cells, levels, seed, block_min, block_max)
 
 
 def _check(cond, msg):
