@@ -1,7 +1,8 @@
 // deriv.cuh -- the stencil pass of the split RK4 substep.
 //
 // One CTA takes one field of one (x, y) tile of a block (W x H points, one
-// thread per column, W and H per block) and marches through z.  The planes k .. k+3 of the
+// thread per column, W and H per block) and marches through z, over the whole
+// block or over the planes [k0, k1) of one z-slab of it.  The planes k .. k+3 of the
 // tile plus a 3-cell halo sit in a 5-slot shared-memory ring, filled as the
 // reference's padded copy fh of symmetry_bd (fmisc.f90:877-901): cells at
 // negative indices hold the mirrored value times the field's parity, cells
@@ -52,11 +53,14 @@ static_assert(deriv_planes_fit(kDerivMinEx), "plane buffer too small for a tile 
 
 // substep tile of the split form's pointwise pass
 constexpr int kPointwiseTile = 128;
+// fewest planes of a z-slab of the stencil pass (each slab pays a 7-plane prologue)
+constexpr int kMinSlab = 8;
 
 struct DerivItem {
   int block;   // index into the level's StepBlock table
   int x0, y0;  // tile origin (array indices)
   int field;
+  int k0 = 0, k1 = 0;   // planes [k0, k1) of the march; k1 == 0: the whole block
 };
 
 // kind of a field's stencil record: 0 gradient + Hessian + adv, 1 gradient + adv, 2 adv
@@ -157,9 +161,10 @@ __device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, i
 // of the D array.
 template <typename A, int KIND, typename T, typename S, typename SI>
 __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, const double* bsh,
-                                             int F, int x0, int y0, T* D, long long dfs, A* ring) {
+                                             int F, int x0, int y0, int k0, int k1, T* D, long long dfs, A* ring) {
   const Coef<A>& C = pick<A>(B.C);
   const int ex0 = B.b.ex[0], ex1 = B.b.ex[1], ex2 = B.b.ex[2];
+  const int kend = k1 > 0 ? k1 : ex2;
   const long long fs = B.b.fs;
   const int W = B.dw, H = DTHREADS / W;
   const int DSX = W + 6;                     // row stride of the plane buffer
@@ -189,15 +194,15 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
   auto dx2 = [&](const A* q) { return C.d2[0] * (-q[-1] + q[1]); };
   auto dy2 = [&](const A* q) { return C.d2[1] * (-q[-DSX] + q[DSX]); };
 
-  // prologue: the loads of planes -3 .. 3 are issued together, then the planes
-  // enter the ring one at a time; the column gets -3 .. 3 and the derivative
-  // windows planes -2 .. 1
+  // prologue: the loads of planes k0-3 .. k0+3 are issued together, then the
+  // planes enter the ring one at a time; the column gets k0-3 .. k0+3 and the
+  // derivative windows planes k0-2 .. k0+1
   A pro[7][DPER];
 #pragma unroll
-  for (int m = -3; m <= 3; ++m) P.fetch_to(m, pro[m + 3]);
+  for (int m = -3; m <= 3; ++m) P.fetch_to(k0 + m, pro[m + 3]);
 #pragma unroll
   for (int m = -3; m <= 3; ++m) {
-    A* slot = ring + ring_slot(m) * DPLANE;
+    A* slot = ring + ring_slot(k0 + m) * DPLANE;
     P.store_from(slot, np, pro[m + 3]);
     __syncthreads();
     const A* q = slot + own;
@@ -219,14 +224,14 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
   }
 
 #pragma unroll 1
-  for (int k = 0; k < ex2; ++k) {
+  for (int k = k0; k < kend; ++k) {
     P.fetch(k + 4);   // in flight while plane k is computed
 #if AMSS_DERIV_PREFETCH
     {
       // warp 0 asks L2 for the tile rows (with halo) of plane k+4+AMSS_DERIV_PREFETCH,
       // one 128-byte line per lane, so the register fetch of that plane meets L2
       const int kk = k + 4 + AMSS_DERIV_PREFETCH;
-      if (threadIdx.x < 32 && kk < ex2) {
+      if (threadIdx.x < 32 && kk < ex2 && kk < kend + 3) {
         const int xl = x0 - 3 < 0 ? 0 : x0 - 3, xh = x0 + W + 3 > ex0 ? ex0 : x0 + W + 3;
         const int yl = y0 - 3 < 0 ? 0 : y0 - 3, yh = y0 + H + 3 > ex1 ? ex1 : y0 + H + 3;
         const int lpr = (int)(((xh - xl) * sizeof(S) + 127) / 128);   // lines per row
@@ -363,16 +368,16 @@ __global__ void __launch_bounds__(DTHREADS, 2) k_deriv(const StepBlock<T>* __res
         // wide fields of the mixed form: FP64 source (state, or the FP64 side stage) and arithmetic
         const double* src = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F) * fs
                                             : (const double*)in + F * fs;
-        deriv_column<double, 0>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<double*>(smem));
+        deriv_column<double, 0>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<double*>(smem));
         __syncthreads();
         continue;
       }
     }
     const SI* src = in + F * fs;
     switch (dkind(F)) {
-      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
-      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
-      default: deriv_column<T, 2>(B, src, in, bsh, F, it.x0, it.y0, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
+      default: deriv_column<T, 2>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
     }
     __syncthreads();
   }
