@@ -223,6 +223,16 @@ int amss_engine_commit(amss_engine* e);
 /* Copy one block's 24-field state (host, Fortran order, field-major) in/out. */
 int amss_engine_set_state(amss_engine* e, int block, const double* host_state);
 int amss_engine_get_state(amss_engine* e, int block, double* host_state);
+/* A block's state `back` level steps before the current one (back 0..2; 0 is
+ * amss_engine_set/get_state), for checkpoints (checkpoint::writecheck_cgh
+ * stores StateList and OldStateList, checkpoint.C:132-190, bssn_class.C:682-683)
+ * and regrids. */
+int amss_engine_set_time_level(amss_engine* e, int block, int back, const double* host_state);
+int amss_engine_get_time_level(amss_engine* e, int block, int back, double* host_state);
+/* Steps a level has taken (the time interpolation of its children is quadratic
+ * from the second step on), and setting it when a run resumes from a checkpoint. */
+int amss_engine_level_clock(amss_engine* e, int level, int* steps);
+int amss_engine_set_level_clock(amss_engine* e, int level, int steps);
 /* Device pointer of field 0 of a block's state and the field stride in elements. */
 int amss_engine_state_device(amss_engine* e, int block, double** dptr, long long* field_stride);
 
@@ -267,6 +277,32 @@ int amss_engine_step_level(amss_engine* e, int level, double dt);
 /* Capture `nsteps` calls of amss_engine_step_level(level, dt) as one CUDA
  * graph and replay it `replays` times. */
 int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int replays);
+
+/* No counterpart in the reference (its work split is the MPI block layout).
+ * Tiling of the stencil pass of one level, the knob amss_b200.autotune
+ * searches: x-y tile width (8..64 columns, H = 256 / width rows; 0 restores
+ * the default, the block's x extent cut into pieces of at most 64) and the
+ * number of z-slabs each block's march is cut into (1..16; slabs are at least
+ * 8 planes).  Results do not depend on it.  Waits for the engine's stream;
+ * not inside a stream capture. */
+int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_w, int zsplit);
+/* The level's tiling (as set; 0 = default width) and its stencil work items. */
+int amss_engine_get_level_tiling(amss_engine* e, int level, int* tile_w, int* zsplit, int* nitems);
+
+/* Moving-box regrid (cgh::Regrid_Onelevel, cgh.C:1304-1506, whose data step is
+ * cgh::recompose_cgh_Onelevel and Parallel::fill_level_data, Parallel.C).
+ * `dst` is a committed engine over the new hierarchy (same grid, fields and
+ * precision), `src` the engine it replaces, both at the same time.  For one
+ * level and one time level (back 0: the current state; 1: the one a level
+ * step before), every cell of dst's blocks (ghosts included) that a block of
+ * src's level owns is copied, and every cell outside all of src's patches
+ * (their buffers included) is prolonged (prolong3) from src's parent level:
+ * from its current state for back 0, from its state interpolated in time to
+ * the midpoint of its current and previous levels (average2, Parallel.C
+ * :4383-4441) for back 1, which overwrites the parent's accumulators.  The
+ * level's clock (ring index, steps taken) is copied too.  A cell outside the
+ * old parent's blocks (boxes not nested) fails with AMSS_ERR_ARG. */
+int amss_engine_regrid_fill(amss_engine* dst, amss_engine* src, int level, int back);
 
 /* Wait for the engine's stream; returns 1 if any substep saw a NaN, else 0. */
 int amss_engine_sync(amss_engine* e);

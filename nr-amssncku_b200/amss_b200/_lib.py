@@ -63,6 +63,13 @@ def lib():
     L.amss_engine_get_punctures.argtypes = [ctypes.c_void_p, _DP]
     L.amss_engine_interp_points.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP, ctypes.c_int, _IP, _DP,
                                             _DP, _IP]
+    L.amss_engine_set_level_tiling.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_regrid_fill.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_set_time_level.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP]
+    L.amss_engine_get_time_level.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _DP]
+    L.amss_engine_level_clock.argtypes = [ctypes.c_void_p, ctypes.c_int, _IP]
+    L.amss_engine_set_level_clock.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_get_level_tiling.argtypes = [ctypes.c_void_p, ctypes.c_int, _IP, _IP, _IP]
     L.get_lousto_nbhs_.restype = ctypes.c_int
     L.amss_lousto_vjp.restype = ctypes.c_int
     L.amss_lousto_vjp.argtypes = [_IP, _DP, _DP, _DP, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP]

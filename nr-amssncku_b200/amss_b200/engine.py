@@ -32,6 +32,8 @@ class Engine:
         if formulation not in ("bssn", "z4c"):
             raise AmssError("formulation must be 'bssn' or 'z4c'")
         self.nf = 25 if formulation == "z4c" else 24
+        self.params = dict(precision=precision, symmetry=symmetry, eps=eps, chitiny=chitiny, kernel=kernel,
+                           formulation=formulation)
         prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0, 0 if kernel == "split" else 1,
                       1 if formulation == "z4c" else 0)
         self._h = lib().amss_engine_create(ctypes.byref(prm))
@@ -112,6 +114,30 @@ class Engine:
         check(lib().amss_engine_get_state(self._h, block, out.ctypes.data_as(_DP)), "amss_engine_get_state")
         return out
 
+    def set_time_level(self, block, back, state):
+        """A block's state `back` level steps before the current one (0..2)."""
+        state = np.ascontiguousarray(state, dtype=np.float64)
+        ex = self.blocks[block]
+        if state.shape != (self.nf, ex[2], ex[1], ex[0]):
+            raise AmssError(f"set_time_level: state must have shape {(self.nf, ex[2], ex[1], ex[0])}")
+        check(lib().amss_engine_set_time_level(self._h, block, back, state.ctypes.data_as(_DP)),
+              "amss_engine_set_time_level")
+
+    def get_time_level(self, block, back):
+        ex = self.blocks[block]
+        out = np.empty((self.nf, ex[2], ex[1], ex[0]))
+        check(lib().amss_engine_get_time_level(self._h, block, back, out.ctypes.data_as(_DP)),
+              "amss_engine_get_time_level")
+        return out
+
+    def level_steps(self, level):
+        n = ctypes.c_int()
+        check(lib().amss_engine_level_clock(self._h, level, ctypes.byref(n)), "amss_engine_level_clock")
+        return n.value
+
+    def set_level_steps(self, level, steps):
+        check(lib().amss_engine_set_level_clock(self._h, level, int(steps)), "amss_engine_set_level_clock")
+
     def state_device(self, block):
         ptr = ctypes.c_void_p()
         fs = ctypes.c_longlong()
@@ -124,6 +150,24 @@ class Engine:
 
     def step(self, level, dt):
         check(lib().amss_engine_step_level(self._h, level, dt), "amss_engine_step_level")
+
+    def regrid_fill(self, old, level, back):
+        """Fill `level`, time level `back` (0 current, 1 previous), from the
+        engine this one replaces (amss_engine_regrid_fill)."""
+        check(lib().amss_engine_regrid_fill(self._h, old._h, level, back), "amss_engine_regrid_fill")
+
+    def set_level_tiling(self, level, tile_w=0, zsplit=1):
+        """Stencil-pass tiling of one level (amss_engine_set_level_tiling):
+        tile width 8..64 (0: default) and z-slabs per block."""
+        check(lib().amss_engine_set_level_tiling(self._h, level, int(tile_w), int(zsplit)),
+              "amss_engine_set_level_tiling")
+
+    def level_tiling(self, level):
+        """(tile width as set, z-slabs, stencil work items) of one level."""
+        w, z, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().amss_engine_get_level_tiling(self._h, level, ctypes.byref(w), ctypes.byref(z), ctypes.byref(n)),
+              "amss_engine_get_level_tiling")
+        return w.value, z.value, n.value
 
     def run_graph(self, level, dt, nsteps, replays=1):
         check(lib().amss_engine_run_graph(self._h, level, dt, nsteps, replays), "amss_engine_run_graph")

@@ -172,6 +172,10 @@ def from_boxes(x0, h0, coarse, levels, seed=1, block_min=24, block_max=80):
     rng = np.random.default_rng(seed)
     coarse = tuple(coarse) if np.ndim(coarse) else (int(coarse),) * 3
     H = Hierarchy(x0, h0)
+    # what a regrid rebuilds from: the boxes per level before merging (one per
+    # puncture, as the reference keeps cgh::bbox per grid) and the split rule
+    H.grid_boxes = [[[list(lo), list(hi)] for lo, hi in boxes] for boxes in levels]
+    H.build_args = dict(coarse=coarse, seed=seed, block_min=block_min, block_max=block_max)
     H.add_patch(0, (0, 0, 0), coarse, 0, [_splits(0, coarse[d], rng, block_min, block_max) for d in range(3)])
     for lev, boxes in enumerate(levels, start=1):
         for lo, hi in merge_boxes(boxes):

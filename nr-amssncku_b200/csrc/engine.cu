@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
 #include <map>
 #include <string>
 #include <vector>
@@ -149,6 +150,8 @@ struct ELevel {
   int nfaces = 0;
   DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
   int nditems = 0;
+  int tile_w = 0;               // stencil-pass tile width (0: deriv_tile_w of each block's x extent)
+  int zsplit = 1;               // z-slabs per block in the stencil pass
   long long dfs = 0;            // slot stride of D for this level
   int* dregion = nullptr;       // per table block: local [lo, hi) of its owned cells inside its patch
   int cur = 0;                  // host mirror of the ring index
@@ -354,6 +357,45 @@ extern "C" int amss_engine_add_amr_block(amss_engine* e, int level, int patch, c
   return (int)e->blocks.size() - 1;
 }
 
+// Stencil-pass tile width of a block of x extent ex0 on level L: the level's
+// tuned width where one is set (at most the block's extent), else deriv_tile_w.
+static int level_tile_w(const ELevel& L, int ex0) {
+  return L.tile_w > 0 ? std::min(L.tile_w, ex0) : deriv_tile_w(ex0);
+}
+
+// Stencil-pass work items of a level: one per (field, x-y tile, z-slab),
+// field-major and grouped by stencil kind (the FP64 fields of the mixed form
+// first), so resident CTAs of the stencil pass run the same code.  A block's
+// z extent is cut into L.zsplit slabs of near-equal height (each slab marches
+// its own planes after a 7-plane prologue): more, shorter work items for
+// levels whose items would otherwise fill the last wave of CTAs poorly.
+static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L) {
+  static const int order[25] = {F_CHI, F_LAP, F_BETAX, F_BETAY, F_BETAZ, F_GXX, F_GXY, F_GXZ,
+                                F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
+                                F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
+  std::vector<DerivItem> tiles;
+  for (size_t m = 0; m < L.blocks.size(); ++m) {
+    const EBlock& b = e->blocks[L.blocks[m]];
+    const int tw = level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
+    const int ns = std::max(1, std::min(L.zsplit, b.ex[2] / kMinSlab));
+    for (int z = 0; z < ns; ++z) {
+      const int k0 = ns == 1 ? 0 : (int)((long long)b.ex[2] * z / ns);
+      const int k1 = ns == 1 ? 0 : (int)((long long)b.ex[2] * (z + 1) / ns);
+      for (int y0 = 0; y0 < b.ex[1]; y0 += th)
+        for (int x0 = 0; x0 < b.ex[0]; x0 += tw) tiles.push_back(DerivItem{(int)m, x0, y0, 0, k0, k1});
+    }
+  }
+  std::vector<DerivItem> items;
+  for (int f : order) {
+    if (f == F_TZ && e->nf != NFIELDS_Z4C) continue;
+    for (DerivItem it : tiles) {
+      it.field = f;
+      items.push_back(it);
+    }
+  }
+  return items;
+}
+
 template <typename T>
 static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<StepBlock<T>> tab;
@@ -366,9 +408,6 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     StepBlock<T> s{};
     s.doff = doff;
     doff += b.fs;
-    const int tw = deriv_tile_w(b.ex[0]), th = deriv_tile_h(b.ex[0]);
-    for (int y0 = 0; y0 < b.ex[1]; y0 += th)
-      for (int x0 = 0; x0 < b.ex[0]; x0 += tw) items.push_back(DerivItem{(int)m, x0, y0, 0});
     s.b.ex[0] = b.ex[0]; s.b.ex[1] = b.ex[1]; s.b.ex[2] = b.ex[2];
     s.b.fs = b.fs;
     s.b.X = b.dX; s.b.Y = b.dX + b.ex[0]; s.b.Z = b.dX + b.ex[0] + b.ex[1];
@@ -389,7 +428,7 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     s.npts = b.npts;
     s.lev0 = level == 0 ? 1 : 0;
     s.nf = e->nf;
-    s.dw = deriv_tile_w(b.ex[0]);
+    s.dw = level_tile_w(L, b.ex[0]);
     if (b.lowsym) L.symm = true;
     tab.push_back(s);
     // substep tiles: kPointwiseTile points for the split form's pointwise pass, 128 for the fused kernel
@@ -407,23 +446,7 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
           }
     }
   }
-  {
-    // one item per (field, tile), field-major and grouped by stencil kind
-    // (the FP64 fields of the mixed form first), so resident CTAs of the
-    // stencil pass run the same code
-    static const int order[25] = {F_CHI, F_LAP, F_BETAX, F_BETAY, F_BETAZ, F_GXX, F_GXY, F_GXZ,
-                                  F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
-                                  F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
-    std::vector<DerivItem> tiles_only;
-    tiles_only.swap(items);
-    for (int f : order) {
-      if (f == F_TZ && e->nf != NFIELDS_Z4C) continue;
-      for (DerivItem it : tiles_only) {
-        it.field = f;
-        items.push_back(it);
-      }
-    }
-  }
+  items = deriv_items(e, L);
   L.ntiles = (int)tiles.size();
   {
     // constraint-norm region of each table block, in array indices.  A block
@@ -668,6 +691,50 @@ extern "C" int amss_engine_get_state(amss_engine* e, int block, double* h) {
   return 0;
 }
 
+// The time level `back` steps behind the current state of a block's level (0..2).
+static double* time_level(amss_engine* e, const EBlock& b, int back) {
+  return b.tl[(e->levels[b.level].cur + 3 - back) % 3];
+}
+
+extern "C" int amss_engine_set_time_level(amss_engine* e, int block, int back, const double* h) {
+  if (int rc = check_block(e, block)) return rc;
+  if (back < 0 || back > 2) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_time_level: back must be 0..2");
+  EBlock& b = e->blocks[block];
+  AMSS_CK(cudaMemcpy2DAsync(time_level(e, b, back), b.fs * sizeof(double), h, b.npts * sizeof(double),
+                            b.npts * sizeof(double), e->nf, cudaMemcpyHostToDevice, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+extern "C" int amss_engine_get_time_level(amss_engine* e, int block, int back, double* h) {
+  if (int rc = check_block(e, block)) return rc;
+  if (back < 0 || back > 2) return amss_fail(AMSS_ERR_ARG, "amss_engine_get_time_level: back must be 0..2");
+  EBlock& b = e->blocks[block];
+  AMSS_CK(cudaMemcpy2DAsync(h, b.npts * sizeof(double), time_level(e, b, back), b.fs * sizeof(double),
+                            b.npts * sizeof(double), e->nf, cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+extern "C" int amss_engine_level_clock(amss_engine* e, int level, int* steps) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_level_clock: no such level");
+  if (steps) *steps = (int)it->second.steps;
+  return 0;
+}
+
+extern "C" int amss_engine_set_level_clock(amss_engine* e, int level, int steps) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end() || steps < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_clock: bad level or steps");
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  it->second.steps = steps;
+  const int st = steps;
+  AMSS_CK(cudaMemcpy(e->dlvl + 2 * level + 1, &st, sizeof(int), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 extern "C" int amss_engine_state_device(amss_engine* e, int block, double** dptr, long long* fs) {
   if (int rc = check_block(e, block)) return rc;
   *dptr = cur_state(e, e->blocks[block]);
@@ -799,6 +866,160 @@ static int recursive_step(amss_engine* e, int l, double dt0) {
     if (l > 0)
       if (int rc = restrict_prolong(e, l, yn)) return rc;
   }
+  return 0;
+}
+
+template <typename T>
+static int patch_table_dw(amss_engine* e, ELevel& L) {
+  for (size_t m = 0; m < L.blocks.size(); ++m) {
+    const int dw = level_tile_w(L, e->blocks[L.blocks[m]].ex[0]);
+    char* dst = (char*)L.dtable + m * sizeof(StepBlock<T>) + offsetof(StepBlock<T>, dw);
+    AMSS_CK(cudaMemcpy(dst, &dw, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_w, int zsplit) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_tiling: no such level");
+  if (tile_w != 0 && (tile_w < kDerivMinEx || tile_w > DWMAX))
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_tiling: tile width must be 0 or 8..64");
+  if (zsplit < 1 || zsplit > 16) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_tiling: zsplit must be 1..16");
+  ELevel& L = it->second;
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  L.tile_w = tile_w;
+  L.zsplit = zsplit;
+  const std::vector<DerivItem> items = deriv_items(e, L);
+  if (L.ditems) cudaFree(L.ditems);
+  L.ditems = nullptr;
+  AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
+  AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  L.nditems = (int)items.size();
+  return e->prm.precision == 1 ? patch_table_dw<float>(e, L) : patch_table_dw<double>(e, L);
+}
+
+extern "C" int amss_engine_get_level_tiling(amss_engine* e, int level, int* tile_w, int* zsplit, int* nitems) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_get_level_tiling: no such level");
+  if (tile_w) *tile_w = it->second.tile_w;
+  if (zsplit) *zsplit = it->second.zsplit;
+  if (nitems) *nitems = it->second.nditems;
+  return 0;
+}
+
+// ---- regrid: fill a level of a new hierarchy from the engine it replaces ----
+
+// a \ b as disjoint boxes
+static void box_subtract(const Box& a, const Box& b, std::vector<Box>& out) {
+  const Box i = intersect(a, b);
+  if (i.empty()) { out.push_back(a); return; }
+  Box rest = a;
+  for (int d = 0; d < 3; ++d) {
+    if (rest.lo[d] < i.lo[d]) { Box s = rest; s.hi[d] = i.lo[d]; out.push_back(s); rest.lo[d] = i.lo[d]; }
+    if (i.hi[d] < rest.hi[d]) { Box s = rest; s.lo[d] = i.hi[d]; out.push_back(s); rest.hi[d] = i.hi[d]; }
+  }
+}
+
+// The AMR kernels' view of a block; its current state slot is tl[*lvl], so
+// the time level `back` steps behind the current one is presented by
+// rotating the ring (cur = the level's host mirror).
+static AmrBlock amr_view(const amss_engine* e, const EBlock& b, int cur, int back) {
+  AmrBlock a{};
+  for (int d = 0; d < 3; ++d) { a.org[d] = b.org[d]; a.ex[d] = b.ex[d]; }
+  a.fs = b.fs;
+  for (int t = 0; t < 3; ++t) a.tl[t] = b.tl[t];
+  a.tl[cur] = b.tl[(cur + 3 - back) % 3];
+  a.st[0] = b.st[0]; a.st[1] = b.st[1];
+  a.side[0] = b.side[0]; a.side[1] = b.side[1];
+  a.K = b.K;
+  a.lvl = e->dlvl + 2 * b.level;
+  a.nf = e->nf;
+  return a;
+}
+
+extern "C" int amss_engine_regrid_fill(amss_engine* dst, amss_engine* src, int level, int back) {
+  if (!dst || !src || !dst->committed || !src->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (dst == src) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: source and destination are one engine");
+  if (back != 0 && back != 1) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: back must be 0 or 1");
+  if (dst->nf != src->nf || dst->prm.precision != src->prm.precision)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: engines differ in fields or precision");
+  for (int d = 0; d < 3; ++d)
+    if (dst->x0[d] != src->x0[d]) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: grids differ");
+  if (dst->h0 != src->h0) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: grids differ");
+  auto id = dst->levels.find(level), is = src->levels.find(level);
+  if (id == dst->levels.end() || is == src->levels.end())
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: level missing in one engine");
+  ELevel& LD = id->second;
+  ELevel& LS = is->second;
+  AMSS_CK(cudaStreamSynchronize(src->stream));
+  AMSS_CK(cudaStreamSynchronize(dst->stream));
+  // the level keeps its clock (ring index, steps taken)
+  AMSS_CK(cudaMemcpy(dst->dlvl + 2 * level, src->dlvl + 2 * level, 2 * sizeof(int), cudaMemcpyDeviceToDevice));
+  LD.cur = LS.cur;
+  LD.steps = LS.steps;
+  // table: the destination level's blocks, the source level's, the source parent's
+  std::vector<AmrBlock> tab;
+  for (int b : LD.blocks) tab.push_back(amr_view(dst, dst->blocks[b], LD.cur, back));
+  for (int b : LS.blocks) tab.push_back(amr_view(src, src->blocks[b], LS.cur, back));
+  const ELevel* LP = nullptr;
+  if (level > 0) {
+    LP = &src->levels[level - 1];
+    for (int b : LP->blocks) tab.push_back(amr_view(src, src->blocks[b], LP->cur, 0));
+  }
+  const int nD = (int)LD.blocks.size(), nS = (int)LS.blocks.size();
+  // copy: every destination cell (ghosts included) that a source block owns
+  std::vector<AmrBox> cp, pr;
+  for (int i = 0; i < nD; ++i)
+    for (int j = 0; j < nS; ++j)
+      push_box(cp, i, nD + j, intersect(dst->blocks[LD.blocks[i]].array(), src->blocks[LS.blocks[j]].own));
+  // prolong: destination cells outside every source patch (buffers included),
+  // from the source parent block that owns their parent cell
+  for (int i = 0; i < nD; ++i) {
+    std::vector<Box> pieces{dst->blocks[LD.blocks[i]].array()};
+    for (int pid : LS.patches) {
+      std::vector<Box> next;
+      for (const Box& q : pieces) box_subtract(q, src->patches[pid].ext(), next);
+      pieces.swap(next);
+    }
+    for (const Box& q : pieces) {
+      if (!LP) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: level 0 must keep its extent");
+      for (size_t c = 0; c < LP->blocks.size(); ++c) {
+        const Box& o = src->blocks[LP->blocks[c]].own;
+        Box of;
+        for (int d = 0; d < 3; ++d) { of.lo[d] = 2 * o.lo[d]; of.hi[d] = 2 * o.hi[d]; }
+        push_box(pr, i, nD + nS + (int)c, intersect(q, of));
+      }
+    }
+  }
+  AmrBlock* dtab = nullptr;
+  DevBoxes dcp, dpr;
+  int rc = 0;
+  unsigned hs = 0;
+  AMSS_CK(cudaMalloc(&dtab, tab.size() * sizeof(AmrBlock)));
+  AMSS_CK(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(AmrBlock), cudaMemcpyHostToDevice));
+  AMSS_CK(cudaMemsetAsync(dst->dstatus, 0, sizeof(unsigned), dst->stream));
+  if ((rc = upload_boxes(cp, dcp)) == 0 && (rc = upload_boxes(pr, dpr, dst->nf)) == 0) {
+    cudaError_t err = cudaSuccess;
+    if (dcp.ntiles)
+      err = launch_amr_sync(dtab, dcp.boxes, dcp.tiles, dcp.ntiles, BUF_STATE, dst->prm.precision == 1, dst->dstatus,
+                            dst->stream);
+    if (err == cudaSuccess && dpr.ntiles && back == 1)   // the parent between its current and previous levels
+      err = launch_amr_timeinterp(src->dblocks, LP->dti_tiles, LP->nti, dst->stream);
+    if (err == cudaSuccess && dpr.ntiles)
+      err = launch_amr_prolong(dtab, dpr.boxes, dpr.tiles, dpr.ntiles, back, dst->dstatus, dst->stream);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&hs, dst->dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost, dst->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(dst->stream);
+    if (err != cudaSuccess) rc = amss_fail(AMSS_ERR_CUDA, cudaGetErrorString(err));
+  }
+  dcp.release();
+  dpr.release();
+  cudaFree(dtab);
+  if (rc) return rc;
+  if (hs & ST_BAD_ARG)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: a cell to fill lies outside the source's parent blocks "
+                                   "(the new boxes are not nested in the old parent level)");
   return 0;
 }
 

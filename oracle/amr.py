@@ -244,6 +244,132 @@ class OracleHierarchy:
         return self.recursive_step(0, dt0)
 
 
+    # cgh::recompose_cgh_Onelevel + Parallel::fill_level_data -----------------
+    def regrid_fill(self, old, level, back):
+        """Fill `level` of this hierarchy (the new boxes), time level `back`
+        (0: current, 1: one level step before), from the hierarchy `old` it
+        replaces (Parallel.C fill_level_data): cells of this level's arrays
+        that an old block owns are copied; cells outside every old patch
+        (buffers included) are prolonged (prolong3) from the old parent level,
+        in time too for back = 1 (average2 of the parent's three levels, the
+        mean of two before its second step).  The level's clock is copied."""
+        lib = O.lib()
+        H, Ho = self.H, old.H
+        self.cur[level] = old.cur[level]
+        self.steps[level] = old.steps[level]
+        slot = (self.cur[level] + 3 - back) % 3
+        oslot = (old.cur[level] + 3 - back) % 3
+        new_ids = [i for p in H.levels[level] for i in p.blocks]
+        old_ids = [i for p in Ho.levels[level] for i in p.blocks]
+        for d in new_ids:
+            bd = H.blocks[d]
+            alo, ahi = bd.org, tuple(bd.org[k] + bd.ex[k] for k in range(3))
+            for s_ in old_ids:
+                bs = Ho.blocks[s_]
+                r = _isect(alo, ahi, bs.own_lo, bs.own_hi)
+                if r:
+                    self._view(bd, self.blk[d]["U"][slot], *r)[...] = old._view(bs, old.blk[s_]["U"][oslot], *r)
+        if level == 0:
+            return
+        # the parent's source values: current state, or interpolated in time
+        cl = level - 1
+        par_ids = [i for p in Ho.levels[cl] for i in p.blocks]
+        src = {}
+        for cb in par_ids:
+            d_ = old.blk[cb]
+            c = old.cur[cl]
+            if back == 0:
+                src[cb] = d_["U"][c]
+            else:
+                f1, f2, f3 = d_["U"][c], d_["U"][(c + 2) % 3], d_["U"][(c + 1) % 3]
+                if old.steps[cl] >= 2:
+                    t = np.empty_like(f1)
+                    lib.oracle_average2(ctypes.c_long(f1.size), _p(f1), _p(f2), _p(f3), _p(t))
+                else:
+                    t = 0.5 * (f1 + f2)
+                src[cb] = t
+        for d in new_ids:
+            bd = H.blocks[d]
+            pieces = [(bd.org, tuple(bd.org[k] + bd.ex[k] for k in range(3)))]
+            for p in Ho.levels[level]:
+                nxt = []
+                for lo, hi in pieces:
+                    nxt += _subtract(lo, hi, p.ext_lo, p.ext_hi)
+                pieces = nxt
+            farr = self.blk[d]["U"][slot]
+            for lo, hi in pieces:
+                for cb in par_ids:
+                    bc = Ho.blocks[cb]
+                    rr = _isect(lo, hi, tuple(2 * v for v in bc.own_lo), tuple(2 * v for v in bc.own_hi))
+                    if not rr:
+                        continue
+                    for f in range(self.nf):
+                        lib.oracle_prolong3_box(_I3(*bc.ex), _I3(*bc.org), _p(src[cb][f]), _I3(*bd.ex),
+                                                _I3(*bd.org), _p(farr[f]), _I3(*rr[0]), _I3(*rr[1]))
+
+
+def _subtract(alo, ahi, blo, bhi):
+    """The box [alo, ahi) less [blo, bhi), as disjoint boxes."""
+    r = _isect(alo, ahi, blo, bhi)
+    if not r:
+        return [(tuple(alo), tuple(ahi))]
+    out = []
+    lo, hi = list(alo), list(ahi)
+    for d in range(3):
+        if lo[d] < r[0][d]:
+            h2 = list(hi)
+            h2[d] = r[0][d]
+            out.append((tuple(lo), tuple(h2)))
+            lo[d] = r[0][d]
+        if r[1][d] < hi[d]:
+            l2 = list(lo)
+            l2[d] = r[1][d]
+            out.append((tuple(l2), tuple(hi)))
+            hi[d] = r[1][d]
+    return out
+
+
+def regrid_onelevel(lev, boxes, handles, porgls, porg0, x0, h0, symmetry=0):
+    """cgh::Regrid_Onelevel's box move (cgh.C:1340-1470) for one level:
+    boxes[grd] = [lo, hi] in the level's global cells (moved in place),
+    handles[grd] their centres (moved in place), porgls[bh] the punctures'
+    positions at the level's last regrid, porg0[bh] the current ones.
+    Returns (moved, new porgls)."""
+    do_every = 2
+    nbh = len(porg0)
+    dX = h0 * 0.5 ** lev
+    tmp = [list(p) for p in porgls]
+    tot_flag = False
+    for grd in range(len(boxes)):
+        bhi = 0
+        while bhi < nbh:
+            if (abs(porgls[bhi][0] - handles[grd][0]) < 2 * do_every * dX and
+                    abs(porgls[bhi][1] - handles[grd][1]) < 2 * do_every * dX and
+                    abs(porgls[bhi][2] - handles[grd][2]) < 2 * do_every * dX):
+                break
+            bhi += 1
+        if bhi == nbh:
+            blo = [x0 + boxes[grd][0][d] * dX for d in range(3)]
+            if abs(blo[0]) < dX / 2 and abs(blo[1]) < dX / 2 and abs(blo[2]) < dX / 2:
+                break
+            if nbh == 1:
+                bhi = 0
+            else:
+                raise ValueError("no black hole matches the box")
+        for d in range(3):
+            rr = (porg0[bhi][d] - handles[grd][d]) / dX
+            flag = int(rr + 0.5) if rr > 0 else int(rr - 0.5)       # Python int() truncates like C
+            flag = int(flag / do_every) * do_every
+            shift = flag * dX
+            if abs(shift) > dX / 2:
+                tot_flag = True
+                boxes[grd][0][d] += flag
+                boxes[grd][1][d] += flag
+                handles[grd][d] += shift
+                tmp[bhi][d] = porg0[bhi][d]
+    return tot_flag, (tmp if tot_flag else porgls)
+
+
 def grid_noise(level, field, gi, gj, gk, seed):
     """Uniform noise in [-1, 1) as a function of (seed, level, field, global
     cell index) only, so every copy of a cell (owner, ghost, buffer) agrees.
