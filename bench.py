@@ -208,10 +208,19 @@ def time_engine(args, w, init, precision, rank, world, dev):
 
     H = w["H"]
     dt0 = w["courant"] * H.h0
+    tiling = {}
+    if args.tune and args.kernel == "split":
+        # the stencil pass's tiling per level, measured on a scratch engine
+        # before anything is timed (amss_b200.autotune)
+        from amss_b200 import autotune
+        tiling = autotune.tune(H, init, dt0, precision=precision, formulation=args.formulation, eps=w["eps"],
+                               cache=args.tune_cache or None)
     eng = amss_b200.Engine.from_hierarchy(H, precision=precision, eps=w["eps"], kernel=args.kernel,
                                           formulation=args.formulation)
     for i, st in enumerate(init):
         eng.set_state(i, st)
+    for lv, (tw, zs, _) in tiling.items():
+        eng.set_level_tiling(lv, tw, zs)
     eng.set_punctures(w["pos"])   # Step tracks the punctures on the finest level (MAPBH 0)
     stream = torch.cuda.ExternalStream(eng.stream)
 
@@ -265,7 +274,8 @@ def time_engine(args, w, init, precision, rank, world, dev):
     e2e_ms = max_over_ranks((t1 - t0) * 1e3 / e2e_steps, world)
     eng.close()
     return dict(ms_per_step=ms / args.steps, e2e_ms=e2e_ms, launches=launches, clocks=clk.summary(),
-                nan=bool(nan), tracked=tracked)
+                nan=bool(nan), tracked=tracked,
+                tiling={str(lv): [tw, zs, round(t, 4)] for lv, (tw, zs, t) in tiling.items()})
 
 
 def roofline(precision, nf, zones, ms_per_step, npts, peak):
@@ -330,6 +340,9 @@ def run_ours(args, rank, world):
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "nan": r["nan"],
+        "tiling": {"per_level": r["tiling"], "what": "stencil-pass tile width (0 = default) and z-slabs per block, "
+                                                    "and the tuner's ms per level step, chosen by amss_b200.autotune "
+                                                    "before the timed region"},
         "punctures_after_warmup_and_timed_steps": r["tracked"],
     }
     if args.precision == "fp64" and args.formulation == "bssn" and not args.no_parts:
@@ -342,7 +355,8 @@ def run_ours(args, rank, world):
                          "e2e": job_rate(zones, world, m["e2e_ms"]), "roofline_frac": mrf["frac"],
                          "roofline_achieved": mrf["achieved"],
                          "algorithmic_bytes_per_zone_update": mrf["algorithmic_bytes_per_zone_update"],
-                         "gpu_launches": int(m["launches"]), "clocks": m["clocks"], "nan": m["nan"]}
+                         "gpu_launches": int(m["launches"]), "clocks": m["clocks"], "nan": m["nan"],
+                         "tiling": m["tiling"]}
         line["mixed_over_fp64"] = ms_per_step / m["ms_per_step"]
         if world == 1:
             a = run_adjoint(args, steps=1, warmup=1)
@@ -589,6 +603,8 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="replay the timed steps as one CUDA graph")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", type=int, default=1, help="pick each level's stencil-pass tiling with the autotuner")
+    ap.add_argument("--tune-cache", default="", help="JSON cache of tuned tilings (default: none, tune every run)")
     ap.add_argument("--no-parts", action="store_true",
                     help="FP64 line only: skip the mixed-form and adjoint parts of the metric")
     ap.add_argument("--report", choices=["none", "mixed"], default="none",

@@ -8,7 +8,8 @@
 // loads it.
 //
 // gpu_rhs takes its scalars by C++ reference; this shim gives ctypes a plain
-// extern "C" symbol with pointers in the same order, and supplies the
+// extern "C" symbol with pointers in the same order (after gpu_rhs's
+// `calledby`, which selects the outputs it copies back), and supplies the
 // reference's result-dump hook compare_result (bssn_macro.h:90, defined in
 // bssn_macro.C:78 against Fortran dump files the reference does not ship),
 // which gpu_rhs only calls under RESULT_CHECK.
@@ -17,7 +18,7 @@
 int compare_result(int, double*, int) { return 0; }
 
 extern "C" int ref_gpu_rhs(
-    int* ex, double* T, double* X, double* Y, double* Z, double* chi, double* trK, double* dxx, double* gxy,
+    int calledby, int* ex, double* T, double* X, double* Y, double* Z, double* chi, double* trK, double* dxx, double* gxy,
     double* gxz, double* dyy, double* gyz, double* dzz, double* Axx, double* Axy, double* Axz, double* Ayy,
     double* Ayz, double* Azz, double* Gamx, double* Gamy, double* Gamz, double* Lap, double* betax, double* betay,
     double* betaz, double* dtSfx, double* dtSfy, double* dtSfz, double* chi_rhs, double* trK_rhs, double* gxx_rhs,
@@ -31,8 +32,9 @@ extern "C" int ref_gpu_rhs(
     double* Gamzyz, double* Gamzzz, double* Rxx, double* Rxy, double* Rxz, double* Ryy, double* Ryz, double* Rzz,
     double* ham_Res, double* movx_Res, double* movy_Res, double* movz_Res, double* Gmx_Res, double* Gmy_Res,
     double* Gmz_Res, int* Symmetry, int* Lev, double* eps, int* co) {
-  // calledby 0 (CALLED_BY_STEP, bssn_macro.h:69): the right-hand sides are copied back
-  return gpu_rhs(0, 0, ex, *T, X, Y, Z, chi, trK, dxx, gxy, gxz, dyy, gyz, dzz, Axx, Axy, Axz, Ayy, Ayz, Azz,
+  // calledby (bssn_macro.h:69-70): 0, CALLED_BY_STEP, copies the right-hand sides back;
+  // 1, CALLED_BY_CONSTRAINT, the Christoffel symbols, Ricci components and residuals
+  return gpu_rhs(calledby, 0, ex, *T, X, Y, Z, chi, trK, dxx, gxy, gxz, dyy, gyz, dzz, Axx, Axy, Axz, Ayy, Ayz, Azz,
                  Gamx, Gamy, Gamz, Lap, betax, betay, betaz, dtSfx, dtSfy, dtSfz, chi_rhs, trK_rhs, gxx_rhs,
                  gxy_rhs, gxz_rhs, gyy_rhs, gyz_rhs, gzz_rhs, Axx_rhs, Axy_rhs, Axz_rhs, Ayy_rhs, Ayz_rhs,
                  Azz_rhs, Gamx_rhs, Gamy_rhs, Gamz_rhs, Lap_rhs, betax_rhs, betay_rhs, betaz_rhs, dtSfx_rhs,

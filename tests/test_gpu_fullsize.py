@@ -8,7 +8,7 @@ libamss_b200.so against the CPU oracle on the same inputs).
   (+-3, 0, 0), 20 uneven blocks): one whole Berger-Oliger coarse step with the
   puncture tracking, graph replay against the oracle hierarchy, <= 1e-12 per
   field over all blocks (trK 5e-12: 112 fine steps of accumulated rounding on
-  a small field), tracked positions bit-identical.
+  a small field), tracked positions equal to 1e-12.
 * adjoint96 (96^3 interior on [-12, 12]^3, BL m = 1 at (0.1, 0.05, 0.02) +
   Gaussian on gamma~_xx): the gradient of sum H^2 dV after 40 FP64 steps with
   a checkpoint every 20 (two segments) against central differences (h = 1e-6)
@@ -85,7 +85,9 @@ def test_amr_workload_one_coarse_step_with_tracking():
     bar = np.full(24, 1e-12)
     bar[1] = 5e-12
     assert np.all(errs <= bar), errs
-    assert np.array_equal(np.asarray(got_pos), np.asarray(oh.porg0))
+    # the positions follow the shift, which differs from the oracle's by the
+    # rounding above: equal to 1e-12 (the y and z components stay ~1e-20)
+    assert np.abs(np.asarray(got_pos) - np.asarray(oh.porg0)).max() <= 1e-12
 
 
 def test_adjoint96_gradient_against_finite_differences():

@@ -39,6 +39,14 @@ TOL = 1e-12
 
 
 def _port(X, Y, Z, st, eps, co, symmetry=0):
+    """gpu_rhs twice: called as the step (the right-hand sides come back)
+    and as the constraint output (the Christoffels, Ricci and residuals)."""
+    rhs = _port_call(0, X, Y, Z, st, eps, co, symmetry)[0]
+    aux = _port_call(1, X, Y, Z, st, eps, co, symmetry)[1:]
+    return [rhs] + aux
+
+
+def _port_call(calledby, X, Y, Z, st, eps, co, symmetry=0):
     lib = ctypes.CDLL(LIB)
     P = ctypes.POINTER(ctypes.c_double)
     st = np.ascontiguousarray(st)
@@ -47,7 +55,8 @@ def _port(X, Y, Z, st, eps, co, symmetry=0):
     matter = np.zeros((10,) + shp)
     p = lambda a: a.ctypes.data_as(P)   # noqa: E731
     X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
-    args = [(ctypes.c_int * 3)(shp[2], shp[1], shp[0]), ctypes.byref(ctypes.c_double(0.0)), p(X), p(Y), p(Z)]
+    args = [ctypes.c_int(calledby), (ctypes.c_int * 3)(shp[2], shp[1], shp[0]), ctypes.byref(ctypes.c_double(0.0)),
+            p(X), p(Y), p(Z)]
     args += [p(st[f]) for f in range(24)] + [p(out[0][f]) for f in range(24)]
     args += [p(matter[f]) for f in range(10)]
     args += [p(a[f]) for a in out[1:] for f in range(a.shape[0])]
