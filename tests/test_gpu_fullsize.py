@@ -122,13 +122,16 @@ def test_adjoint96_gradient_against_finite_differences():
     eps = 1e-6
     drng = np.random.default_rng(8)
     # the gamma~_xx field along a smooth seeded direction (a Gaussian of width 2
-    # at a second random centre times a seeded plane wave): at 96^3 a grid-scale
-    # random field direction changes L by less than L's own rounding over
-    # 40 steps divided by h (measured: 3e-5 relative), so it cannot test the
-    # gradient; then mass and position together
+    # at a second random centre times a seeded plane wave) of amplitude 100, so
+    # that h v is of the bump's own size (1e-4): L = 0.31 moves by only ~2e-3 h
+    # per unit of this direction, and for h v ~ 1e-6 that change is below the
+    # rounding L accumulates over 40 steps of 1e6 points (measured relative
+    # error 1.9e-5 at h v = 1e-6, 8.9e-5 at 1e-7, 4e-8 at 1e-4: the 1/h
+    # signature of rounding); then mass and position together
     z, y, x = np.meshgrid(X, X, X, indexing="ij")
     c2, k = drng.uniform(-3.0, 3.0, 3), drng.uniform(0.3, 0.8, 3)
-    vfield = np.exp(-((x - c2[0]) ** 2 + (y - c2[1]) ** 2 + (z - c2[2]) ** 2) / 4.0) * np.sin(k[0] * x + k[1] * y + k[2] * z)
+    vfield = 100.0 * np.exp(-((x - c2[0]) ** 2 + (y - c2[1]) ** 2 + (z - c2[2]) ** 2) / 4.0) * \
+        np.sin(k[0] * x + k[1] * y + k[2] * z)
     directions = [
         (np.zeros(1), np.zeros((1, 3)), vfield),
         (drng.standard_normal(1), drng.standard_normal((1, 3)), np.zeros(bump.shape)),
