@@ -356,6 +356,73 @@ int amss_engine_set_punctures(amss_engine* e, int n, const double* pos);
  * for the engine's stream. */
 int amss_engine_get_punctures(amss_engine* e, double* pos);
 
+/* ---- Blocks divided among ranks, one engine per GPU (Parallel::distribute,
+ * Parallel.C:504-827, assigns the reference's blocks to MPI ranks;
+ * Parallel::Sync / transfer, Parallel.C:3677-3776 and :3508-3592, move the
+ * ghost, restriction and prolongation segments between them).
+ *
+ * Every rank builds the same hierarchy (same blocks in the same order) and
+ * names the owner of each block before amss_engine_commit; an engine then
+ * allocates and steps only its own blocks.  Each transfer (the ghost sync of
+ * a level after every substep and step, the restriction into and the
+ * prolongation from the parent after a fine step) runs on the rank that owns
+ * the source block, into the destination block or, when another rank owns
+ * that, into a staging region that the exchange delivers and the receiver
+ * copies in.  The results are those of one engine holding every block, bit
+ * for bit.  A rank engine refuses what needs the whole hierarchy
+ * (graph capture, puncture tracking, point interpolation, regrid) with
+ * AMSS_ERR_UNSUPPORTED; its constraint sums cover its own blocks. */
+
+/* Before commit: this engine is `rank` of `nranks` (default 0 of 1), then
+ * the owner of each block (default 0). */
+int amss_engine_set_rank(amss_engine* e, int rank, int nranks);
+int amss_engine_set_block_owner(amss_engine* e, int block, int owner);
+
+/* Transport 1, ranks in one process (one host thread per rank, each with its
+ * engine's device current): create a group of nranks, join every committed
+ * rank engine, then step all ranks concurrently.  At each exchange the ranks
+ * meet at a host barrier; one that does not arrive within timeout_s seconds
+ * fails every rank's step with AMSS_ERR_STATE and the group stays failed.
+ * Destroy the engines before the group. */
+typedef struct amss_group amss_group;
+amss_group* amss_group_create(int nranks, double timeout_s);
+void amss_group_destroy(amss_group* g);
+int amss_group_join(amss_engine* e, amss_group* g);
+int amss_group_barrier(amss_group* g);   /* the exchange's host barrier alone */
+
+/* Transport 2, NCCL (one process per GPU): rank 0 makes a unique id (128
+ * bytes), the caller broadcasts it, every rank passes it after commit
+ * (collective, ncclCommInitRank).  The exchange is a grouped ncclSend /
+ * ncclRecv on the engine's stream.  libnccl.so.2 is opened at run time. */
+int amss_nccl_unique_id(unsigned char id[128]);
+int amss_engine_set_nccl(amss_engine* e, const unsigned char id[128]);
+
+/* The unsquared sums behind amss_engine_constraint_norms (whose values are
+ * their square roots) over this engine's blocks: the ranks add them up. */
+int amss_engine_constraint_sums(amss_engine* e, int level, double sums[8]);
+
+/* Transfer plans without a device (for checking a partition on any host):
+ * amss_plan_create takes the parameters of amss_engine_create; add blocks,
+ * ranks and owners as for an engine, then amss_plan_commit.  The plan
+ * queries below work on plans and committed engines alike. */
+amss_engine* amss_plan_create(const amss_params* prm);
+int amss_plan_commit(amss_engine* e);
+int amss_engine_xfer_count(amss_engine* e);
+/* info: kind (0 ghost sync, 1 restriction, 2 prolongation), level (the fine
+ * level for 1 and 2), boxes over all ranks, boxes crossing ranks, run boxes,
+ * unpack boxes, staging-out bytes, staging-in bytes. */
+int amss_engine_xfer_info(amss_engine* e, int xfer, long long info[8]);
+/* list 0: the boxes this rank's transfer kernel computes; 1: the copies from
+ * received staging blocks.  8 ints per box: dst, src, lo[3], n[3]; block ids
+ * past the hierarchy's are staging blocks.  out NULL: the count. */
+int amss_engine_xfer_boxes(amss_engine* e, int xfer, int list, int* out, int cap);
+/* dir 0: send, 1: receive; 3 values per peer: rank, byte offset, bytes. */
+int amss_engine_xfer_peers(amss_engine* e, int xfer, int dir, long long* out, int cap);
+/* A staging block: org[3], ex[3], byte offset, arena (0 out, 1 in).  Its
+ * buffers start at the offset: nf FP64 fields of ex points, or the stage
+ * fields (FP32 in the mixed form, then 5 FP64 side fields 256-byte aligned). */
+int amss_engine_staging_block(amss_engine* e, int id, long long out[8]);
+
 /* ---- Adjoint of a single-patch BSSN evolution (no reference counterpart:
  * the reference has no derivative code; the forward it differentiates is the
  * level-0 RK4 step of bssn_class::Step, bssn_class.C:2981-3700, with

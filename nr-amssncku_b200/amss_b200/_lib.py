@@ -85,6 +85,26 @@ def lib():
     L.amss_adjoint_stream.argtypes = [ctypes.c_void_p]
     L.amss_adjoint_launch_count.restype = ctypes.c_longlong
     L.amss_adjoint_launch_count.argtypes = [ctypes.c_void_p]
+    L.amss_engine_set_rank.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_set_block_owner.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.amss_group_create.restype = ctypes.c_void_p
+    L.amss_group_create.argtypes = [ctypes.c_int, ctypes.c_double]
+    L.amss_group_destroy.restype = None
+    L.amss_group_destroy.argtypes = [ctypes.c_void_p]
+    L.amss_group_join.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.amss_group_barrier.argtypes = [ctypes.c_void_p]
+    L.amss_nccl_unique_id.argtypes = [ctypes.c_char_p]
+    L.amss_engine_set_nccl.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    L.amss_engine_constraint_sums.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+    L.amss_plan_create.restype = ctypes.c_void_p
+    L.amss_plan_create.argtypes = [ctypes.c_void_p]
+    L.amss_plan_commit.argtypes = [ctypes.c_void_p]
+    L.amss_engine_xfer_count.argtypes = [ctypes.c_void_p]
+    L.amss_engine_xfer_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    L.amss_engine_xfer_boxes.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _IP, ctypes.c_int]
+    L.amss_engine_xfer_peers.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    L.amss_engine_staging_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
     _lib = L
     return L
 

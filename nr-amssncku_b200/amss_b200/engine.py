@@ -28,6 +28,8 @@ class Engine:
     formulation: "bssn" (24 fields) or "z4c" (25 fields, Theta last; split
     kernel only)."""
 
+    _create = "amss_engine_create"
+
     def __init__(self, precision="fp64", symmetry=0, eps=0.1, chitiny=1e-5, kernel="split", formulation="bssn"):
         if formulation not in ("bssn", "z4c"):
             raise AmssError("formulation must be 'bssn' or 'z4c'")
@@ -36,11 +38,12 @@ class Engine:
                            formulation=formulation)
         prm = _Params(1 if precision == "mixed" else 0, symmetry, eps, chitiny - 1.0, 0 if kernel == "split" else 1,
                       1 if formulation == "z4c" else 0)
-        self._h = lib().amss_engine_create(ctypes.byref(prm))
+        self._h = getattr(lib(), self._create)(ctypes.byref(prm))
         if not self._h:
-            raise AmssError("amss_engine_create failed: " + last_error())
+            raise AmssError(f"{self._create} failed: " + last_error())
         self.blocks = []
         self._ntrack = 0
+        self.rank, self.nranks = 0, 1
 
     def close(self):
         if self._h:
@@ -72,9 +75,11 @@ class Engine:
         return bid
 
     @classmethod
-    def from_hierarchy(cls, H, **kw):
-        """An engine holding every block of an amss_b200.hierarchy.Hierarchy,
-        block ids equal to their index in H.blocks."""
+    def from_hierarchy(cls, H, rank=0, nranks=1, owners=None, **kw):
+        """An engine over every block of an amss_b200.hierarchy.Hierarchy,
+        block ids equal to their index in H.blocks.  With nranks > 1 it is
+        rank `rank` of a job whose block owners are `owners` (one rank per
+        block, amss_b200.dist.partition): it holds and steps only its own."""
         e = cls(**kw)
         e.set_grid((H.x0,) * 3, H.h0)
         for lev, patches in enumerate(H.levels):
@@ -83,8 +88,22 @@ class Engine:
                     b = H.blocks[bi]
                     got = e.add_amr_block(lev, pid, b.org, b.ex, b.own_lo, b.own_hi, p.lo, p.hi, p.buffer)
                     assert got == bi
+        if nranks > 1 or rank:
+            e.set_rank(rank, nranks)
+            if owners is None or len(owners) != len(H.blocks):
+                raise AmssError("from_hierarchy: nranks > 1 needs one owner per block")
+            for bi, o in enumerate(owners):
+                e.set_block_owner(bi, int(o))
         e.commit()
         return e
+
+    def set_rank(self, rank, nranks):
+        """This engine is rank `rank` of `nranks` (before commit)."""
+        check(lib().amss_engine_set_rank(self._h, int(rank), int(nranks)), "amss_engine_set_rank")
+        self.rank, self.nranks = int(rank), int(nranks)
+
+    def set_block_owner(self, block, owner):
+        check(lib().amss_engine_set_block_owner(self._h, int(block), int(owner)), "amss_engine_set_block_owner")
 
     def coarse_step(self, dt0):
         check(lib().amss_engine_coarse_step(self._h, dt0), "amss_engine_coarse_step")
@@ -179,6 +198,14 @@ class Engine:
         out = np.zeros(8)
         check(lib().amss_engine_constraint_norms(self._h, level, out.ctypes.data_as(_DP)),
               "amss_engine_constraint_norms")
+        return out
+
+    def constraint_sums(self, level):
+        """The squared sums behind constraint_norms over this engine's own
+        blocks (the ranks of a job add them, then take square roots)."""
+        out = np.zeros(8)
+        check(lib().amss_engine_constraint_sums(self._h, level, out.ctypes.data_as(_DP)),
+              "amss_engine_constraint_sums")
         return out
 
     def interp_points(self, level, points, fields, soa=None):

@@ -22,10 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "amr_types.cuh"
-#include "deriv.cuh"
-#include "dev_util.cuh"
-#include "interp.cuh"
+#include "engine_internal.cuh"
 
 namespace amss {
 
@@ -78,122 +75,10 @@ int check_device(const char* who) {
   return 0;
 }
 
-struct Box {
-  int lo[3], hi[3];
-  bool empty() const { return lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2]; }
-};
-static Box intersect(const Box& a, const Box& b) {
-  Box r;
-  for (int d = 0; d < 3; ++d) {
-    r.lo[d] = std::max(a.lo[d], b.lo[d]);
-    r.hi[d] = std::min(a.hi[d], b.hi[d]);
-  }
-  return r;
-}
-
-struct EPatch {
-  int level;
-  Box phys;            // physical cells
-  int buffer;          // buffer cells each side (0 on level 0)
-  Box ext() const {
-    Box b = phys;
-    for (int d = 0; d < 3; ++d) { b.lo[d] -= buffer; b.hi[d] += buffer; }
-    return b;
-  }
-  std::vector<int> blocks;
-};
-
-struct EBlock {
-  int level = 0, patch = -1;
-  int ex[3], org[3];
-  Box own;
-  long long npts, fs;
-  double bbox[6], pbbox[6];
-  std::vector<double> X, Y, Z;
-  int face_mask = 0, lowsym = 0;
-  bool l2_by_bbox = false;      // added by bbox: its L2-norm cells follow l2normhelper's bbox test
-  double* dX = nullptr;
-  double* tl[3] = {nullptr, nullptr, nullptr};
-  double* K = nullptr;
-  void* st[2] = {nullptr, nullptr};
-  double* side[2] = {nullptr, nullptr};
-  Box array() const {
-    Box b;
-    for (int d = 0; d < 3; ++d) { b.lo[d] = org[d]; b.hi[d] = org[d] + ex[d]; }
-    return b;
-  }
-};
-
-struct DevBoxes {
-  AmrBox* boxes = nullptr;
-  int2* tiles = nullptr;
-  int ntiles = 0;
-  void release() {
-    if (boxes) cudaFree(boxes);
-    if (tiles) cudaFree(tiles);
-    boxes = nullptr;
-    tiles = nullptr;
-  }
-};
-
-struct ELevel {
-  std::vector<int> blocks;
-  std::vector<int> patches;
-  int ntiles = 0;
-  int2* dtiles = nullptr;       // substep tiles (index into this level's table)
-  void* dtable = nullptr;       // StepBlock table
-  bool symm = false;
-  DevBoxes sync, restrict_, prolong;
-  int2* dti_tiles = nullptr;    // time-interpolation tiles (global block ids)
-  int nti = 0;
-  int2* dfaces = nullptr;       // outer-face points (table index, point) for k_face
-  int nfaces = 0;
-  DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
-  int nditems = 0;
-  int tile_w = 0;               // stencil-pass tile width (0: deriv_tile_w of each block's x extent)
-  int zsplit = 1;               // z-slabs per block in the stencil pass
-  long long dfs = 0;            // slot stride of D for this level
-  int* dregion = nullptr;       // per table block: local [lo, hi) of its owned cells inside its patch
-  int cur = 0;                  // host mirror of the ring index
-  long long steps = 0;
-};
-
 }  // namespace amss
 
 using namespace amss;
 
-struct amss_engine {
-  amss_params prm;
-  bool grid_set = false;
-  double x0[3] = {0, 0, 0};
-  double h0 = 1.0;
-  std::vector<EBlock> blocks;
-  std::vector<EPatch> patches;
-  std::map<std::pair<int, int>, int> patch_ids;   // (level, patch) -> index
-  std::map<int, ELevel> levels;
-  cudaStream_t stream = nullptr;
-  unsigned* dstatus = nullptr;
-  int* dlvl = nullptr;          // 2 ints per level: ring index, steps taken
-  AmrBlock* dblocks = nullptr;
-  void* D = nullptr;            // stencil terms of the level being stepped (split form)
-  char* arena = nullptr;
-  size_t arena_bytes = 0;
-  long long launches = 0;
-  bool committed = false;
-  int sm_count = 148;
-  int nf = NFIELDS_BSSN;        // evolved fields: 24 (BSSN) or 25 (Z4c)
-  double* cons = nullptr;       // constraint residuals of a level (7 x its D stride), grow-only
-  long long cons_cap = 0;
-  double* cpart = nullptr;      // per-CTA partial sums of the constraint norms (8 each)
-  int ntrack = 0, track_level = -1;   // puncture tracking on the finest level
-  TrackState* dtrack = nullptr;
-  TrackPatch* dtpatch = nullptr;
-  TrackBlock* dtblock = nullptr;
-  int ntpatch = 0;
-  InterpItem* iitems = nullptr;   // point interpolation: items and results, grow-only
-  double* iout = nullptr;
-  long long icap = 0;
-};
 
 extern "C" const char* amss_last_error(void) { return g_err.c_str(); }
 extern "C" const char* amss_version(void) { return "amss_b200 0.2 (sm_100a)"; }
@@ -221,6 +106,7 @@ extern "C" amss_engine* amss_engine_create(const amss_params* prm) {
   }
   int dev = 0;
   cudaGetDevice(&dev);
+  e->device = dev;
   cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, dev);
   return e;
 }
@@ -228,6 +114,7 @@ extern "C" amss_engine* amss_engine_create(const amss_params* prm) {
 extern "C" void amss_engine_destroy(amss_engine* e) {
   if (!e) return;
   if (e->stream) cudaStreamSynchronize(e->stream);
+  amss_xfer_detach(e);
   for (auto& kv : e->levels) {
     ELevel& L = kv.second;
     if (L.dtiles) cudaFree(L.dtiles);
@@ -236,10 +123,8 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.ditems) cudaFree(L.ditems);
     if (L.dfaces) cudaFree(L.dfaces);
     if (L.dregion) cudaFree(L.dregion);
-    L.sync.release();
-    L.restrict_.release();
-    L.prolong.release();
   }
+  release_xfers(e);
   if (e->dblocks) cudaFree(e->dblocks);
   if (e->D) cudaFree(e->D);
   if (e->dlvl) cudaFree(e->dlvl);
@@ -374,8 +259,8 @@ static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L) {
                                 F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
                                 F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
   std::vector<DerivItem> tiles;
-  for (size_t m = 0; m < L.blocks.size(); ++m) {
-    const EBlock& b = e->blocks[L.blocks[m]];
+  for (size_t m = 0; m < L.own.size(); ++m) {
+    const EBlock& b = e->blocks[L.own[m]];
     const int tw = level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
     const int ns = std::max(1, std::min(L.zsplit, b.ex[2] / kMinSlab));
     for (int z = 0; z < ns; ++z) {
@@ -403,8 +288,8 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<int2> faces;
   std::vector<DerivItem> items;
   long long doff = 0;
-  for (size_t m = 0; m < L.blocks.size(); ++m) {
-    EBlock& b = e->blocks[L.blocks[m]];
+  for (size_t m = 0; m < L.own.size(); ++m) {
+    EBlock& b = e->blocks[L.own[m]];
     StepBlock<T> s{};
     s.doff = doff;
     doff += b.fs;
@@ -454,9 +339,9 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     // lies within one cell of the patch box (l2normhelper, fmisc.f90:1286-1303).
     // An AMR block: its owned cells inside its patch, buffer cells included
     // (the patch box of Parallel::L2Norm holds them, MPatch.C:48-51).
-    std::vector<int> reg(6 * L.blocks.size());
-    for (size_t m = 0; m < L.blocks.size(); ++m) {
-      const EBlock& b = e->blocks[L.blocks[m]];
+    std::vector<int> reg(6 * L.own.size());
+    for (size_t m = 0; m < L.own.size(); ++m) {
+      const EBlock& b = e->blocks[L.own[m]];
       if (b.l2_by_bbox) {
         const std::vector<double>* xs[3] = {&b.X, &b.Y, &b.Z};
         for (int d = 0; d < 3; ++d) {
@@ -474,11 +359,14 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
       }
     }
     if (L.dregion) cudaFree(L.dregion);
-    AMSS_CK(cudaMalloc(&L.dregion, reg.size() * sizeof(int)));
-    AMSS_CK(cudaMemcpy(L.dregion, reg.data(), reg.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!reg.empty()) {
+      AMSS_CK(cudaMalloc(&L.dregion, reg.size() * sizeof(int)));
+      AMSS_CK(cudaMemcpy(L.dregion, reg.data(), reg.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
   }
   L.dfs = doff;
   L.nditems = (int)items.size();
+  if (tab.empty()) return 0;   // a rank without blocks on this level: no step tables
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   AMSS_CK(cudaMalloc(&L.dtable, tab.size() * sizeof(StepBlock<T>)));
@@ -495,7 +383,7 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
 
 // Tiles of 128 work units per box: box cells, or (prolong_nf fields) the
 // (field, run of kProlongRun fine cells along x) units the prolongation counts.
-static int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf = 0) {
+int amss::upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf) {
   std::vector<int2> tiles;
   for (size_t m = 0; m < boxes.size(); ++m) {
     const long long nx = prolong_nf ? prolong_runs_x(boxes[m].lo[0], boxes[m].n[0]) : boxes[m].n[0];
@@ -511,7 +399,7 @@ static int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolo
   return 0;
 }
 
-static void push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b) {
+void amss::push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b) {
   if (b.empty()) return;
   AmrBox a;
   a.dst = dst;
@@ -520,93 +408,48 @@ static void push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b) {
   v.push_back(a);
 }
 
-// Same-level ghost fill (Parallel::Sync, Parallel.C:3677-3776): every cell of a
-// block's array that another block of the level owns is copied from it.
-static std::vector<AmrBox> sync_boxes(amss_engine* e, const ELevel& L) {
-  std::vector<AmrBox> v;
-  for (int d : L.blocks)
-    for (int s : L.blocks)
-      if (d != s) push_box(v, d, s, intersect(e->blocks[d].array(), e->blocks[s].own));
-  return v;
-}
-
-// Restriction (Parallel::Restrict, Parallel.C:4485-4543): every cell of a
-// parent block's array (ghosts included) inside a child patch's physical
-// region, from the child block that owns its two children per direction.
-static std::vector<AmrBox> restrict_boxes(amss_engine* e, const ELevel& F, const ELevel& C) {
-  std::vector<AmrBox> v;
-  for (int pid : F.patches) {
-    const EPatch& P = e->patches[pid];
-    Box cphys;
-    for (int d = 0; d < 3; ++d) { cphys.lo[d] = P.phys.lo[d] / 2; cphys.hi[d] = P.phys.hi[d] / 2; }
-    for (int cb : C.blocks) {
-      const Box r = intersect(cphys, e->blocks[cb].array());
-      if (r.empty()) continue;
-      for (int fb : P.blocks) {
-        const Box& o = e->blocks[fb].own;
-        Box oc;
-        for (int d = 0; d < 3; ++d) { oc.lo[d] = o.lo[d] / 2; oc.hi[d] = o.hi[d] / 2; }
-        push_box(v, cb, fb, intersect(r, oc));
-      }
-    }
-  }
-  return v;
-}
-
-// Prolongation into the buffer cells (Parallel::OutBdLow2Hi,
-// Parallel.C:4589-4689): every cell of a child block's array in its patch's
-// buffer region, from the parent block that owns the cell's parent.
-static std::vector<AmrBox> prolong_boxes(amss_engine* e, const ELevel& F, const ELevel& C) {
-  std::vector<AmrBox> v;
-  for (int pid : F.patches) {
-    const EPatch& P = e->patches[pid];
-    const Box ext = P.ext();
-    std::vector<Box> slabs;
-    for (int d = 0; d < 3; ++d) {
-      Box lo = ext, hi = ext;
-      for (int q = 0; q < d; ++q) { lo.lo[q] = hi.lo[q] = P.phys.lo[q]; lo.hi[q] = hi.hi[q] = P.phys.hi[q]; }
-      lo.hi[d] = P.phys.lo[d];
-      hi.lo[d] = P.phys.hi[d];
-      slabs.push_back(lo);
-      slabs.push_back(hi);
-    }
-    for (int fb : P.blocks)
-      for (const Box& s : slabs) {
-        const Box r = intersect(s, e->blocks[fb].array());
-        if (r.empty()) continue;
-        for (int cb : C.blocks) {
-          const Box& o = e->blocks[cb].own;
-          Box of;
-          for (int d = 0; d < 3; ++d) { of.lo[d] = 2 * o.lo[d]; of.hi[d] = 2 * o.hi[d]; }
-          push_box(v, fb, cb, intersect(r, of));
-        }
-      }
-  }
-  return v;
-}
-
-extern "C" int amss_engine_commit(amss_engine* e) {
-  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: already committed");
-  if (e->blocks.empty()) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: no blocks");
-  const bool mixed = e->prm.precision == 1;
-  const size_t ss = mixed ? sizeof(float) : sizeof(double);
+// Levels 0..L-1 without gaps; each level's owned blocks (every block with one rank).
+static int prepare_levels(amss_engine* e, int* nlev_out) {
   int nlev = 0;
   for (auto& kv : e->levels) nlev = std::max(nlev, kv.first + 1);
   for (int l = 0; l < nlev; ++l)
     if (!e->levels.count(l)) return amss_fail(AMSS_ERR_ARG, "amss_engine_commit: levels must be 0..L-1 without gaps");
+  for (auto& kv : e->levels) {
+    kv.second.own.clear();
+    for (int b : kv.second.blocks)
+      if (e->owned(b)) kv.second.own.push_back(b);
+  }
+  *nlev_out = nlev;
+  return 0;
+}
+
+extern "C" int amss_engine_commit(amss_engine* e) {
+  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: already committed");
+  if (e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: a plan-only engine commits with amss_plan_commit");
+  if (e->blocks.empty()) return amss_fail(AMSS_ERR_STATE, "amss_engine_commit: no blocks");
+  const bool mixed = e->prm.precision == 1;
+  const size_t ss = mixed ? sizeof(float) : sizeof(double);
+  int nlev = 0;
+  if (int rc = prepare_levels(e, &nlev)) return rc;
+  if (int rc = build_xfers(e)) return rc;
+  // arrays of the blocks this rank owns; the others are geometry only
   size_t bytes = 0;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
   for (auto& b : e->blocks) {
+    if (b.owner != e->rank) continue;
     bytes += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
     bytes += align((size_t)e->nf * b.fs * sizeof(double)) * 4;  // 3 time levels + K
     bytes += align((size_t)e->nf * b.fs * ss) * 2;              // two stages
     if (mixed) bytes += align((size_t)kSideFields * b.fs * sizeof(double)) * 2;
   }
-  AMSS_CK(cudaMalloc(&e->arena, bytes));
-  AMSS_CK(cudaMemset(e->arena, 0, bytes));
+  if (bytes) {
+    AMSS_CK(cudaMalloc(&e->arena, bytes));
+    AMSS_CK(cudaMemset(e->arena, 0, bytes));
+  }
   e->arena_bytes = bytes;
   char* p = e->arena;
   for (auto& b : e->blocks) {
+    if (b.owner != e->rank) continue;
     b.dX = (double*)p;
     p += align((size_t)(b.ex[0] + b.ex[1] + b.ex[2]) * sizeof(double));
     for (int t = 0; t < 3; ++t) { b.tl[t] = (double*)p; p += align((size_t)e->nf * b.fs * sizeof(double)); }
@@ -636,38 +479,90 @@ extern "C" int amss_engine_commit(amss_engine* e) {
     a.lvl = e->dlvl + 2 * b.level;
     a.nf = e->nf;
   }
+  if (int rc = upload_xfers(e, ab)) return rc;   // appends the staging blocks to the table
   AMSS_CK(cudaMalloc(&e->dblocks, ab.size() * sizeof(AmrBlock)));
   AMSS_CK(cudaMemcpy(e->dblocks, ab.data(), ab.size() * sizeof(AmrBlock), cudaMemcpyHostToDevice));
   for (auto& kv : e->levels) {
     ELevel& L = kv.second;
     const int rc = mixed ? build_table<float>(e, L, kv.first) : build_table<double>(e, L, kv.first);
     if (rc) return rc;
-    if (int r2 = upload_boxes(sync_boxes(e, L), L.sync)) return r2;
     std::vector<int2> ti;
-    for (int b : L.blocks)
+    for (int b : L.own)
       for (long long q = 0; q < e->blocks[b].npts; q += 128) ti.push_back(make_int2(b, (int)q));
     L.nti = (int)ti.size();
-    AMSS_CK(cudaMalloc(&L.dti_tiles, ti.size() * sizeof(int2)));
-    AMSS_CK(cudaMemcpy(L.dti_tiles, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
-    if (kv.first > 0) {
-      ELevel& C = e->levels[kv.first - 1];
-      if (int r3 = upload_boxes(restrict_boxes(e, L, C), L.restrict_)) return r3;
-      if (int r4 = upload_boxes(prolong_boxes(e, L, C), L.prolong, e->nf)) return r4;
+    if (!ti.empty()) {
+      AMSS_CK(cudaMalloc(&L.dti_tiles, ti.size() * sizeof(int2)));
+      AMSS_CK(cudaMemcpy(L.dti_tiles, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
     }
   }
   if (e->prm.kernel == 0) {
     long long mx = 0;
     for (auto& kv : e->levels) mx = std::max(mx, kv.second.dfs);
     const int slots = e->nf == NFIELDS_Z4C ? D_SLOTS_Z4C : D_SLOTS;
-    AMSS_CK(cudaMalloc(&e->D, (size_t)mx * slots * (mixed ? sizeof(float) : sizeof(double))));
+    if (mx) AMSS_CK(cudaMalloc(&e->D, (size_t)mx * slots * (mixed ? sizeof(float) : sizeof(double))));
+  }
+  if (e->nranks > 1) {
+    AMSS_CK(cudaEventCreateWithFlags(&e->ev_ready, cudaEventDisableTiming));
+    AMSS_CK(cudaEventCreateWithFlags(&e->ev_done, cudaEventDisableTiming));
   }
   e->committed = true;
   return 0;
 }
 
+extern "C" amss_engine* amss_plan_create(const amss_params* prm) {
+  if (!prm) { amss_fail(AMSS_ERR_ARG, "amss_plan_create: null params"); return nullptr; }
+  if (prm->formulation != 0 && prm->formulation != 1) {
+    amss_fail(AMSS_ERR_ARG, "amss_plan_create: formulation must be 0 (BSSN) or 1 (Z4c)");
+    return nullptr;
+  }
+  amss_engine* e = new amss_engine();
+  e->prm = *prm;
+  e->nf = prm->formulation == 1 ? NFIELDS_Z4C : NFIELDS_BSSN;
+  e->plan_only = true;
+  return e;
+}
+
+extern "C" int amss_plan_commit(amss_engine* e) {
+  if (!e || !e->plan_only || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_plan_commit: not an uncommitted plan");
+  if (e->blocks.empty()) return amss_fail(AMSS_ERR_STATE, "amss_plan_commit: no blocks");
+  int nlev = 0;
+  if (int rc = prepare_levels(e, &nlev)) return rc;
+  if (int rc = build_xfers(e)) return rc;
+  e->committed = true;
+  return 0;
+}
+
+extern "C" int amss_engine_set_rank(amss_engine* e, int rank, int nranks) {
+  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_set_rank: engine already committed");
+  if (nranks < 1 || rank < 0 || rank >= nranks) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_rank: need 0 <= rank < nranks");
+  e->rank = rank;
+  e->nranks = nranks;
+  return 0;
+}
+
+extern "C" int amss_engine_set_block_owner(amss_engine* e, int block, int owner) {
+  if (!e || e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_set_block_owner: engine already committed");
+  if (block < 0 || block >= (int)e->blocks.size()) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_block_owner: bad block id");
+  if (owner < 0 || owner >= e->nranks) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_block_owner: owner must be 0..nranks-1");
+  e->blocks[block].owner = owner;
+  return 0;
+}
+
 static int check_block(amss_engine* e, int block) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
   if (block < 0 || block >= (int)e->blocks.size()) return amss_fail(AMSS_ERR_ARG, "bad block id");
+  if (!e->owned(block)) return amss_fail(AMSS_ERR_ARG, "block is owned by another rank");
+  return 0;
+}
+
+// Entry points that need every block on this engine (tracking, point
+// interpolation, regrid, graph capture) refuse an engine that holds a share.
+static int check_whole(amss_engine* e, const char* who) {
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (e->nranks > 1) {
+    std::string m = std::string(who) + ": not available on an engine that holds one rank's blocks";
+    return amss_fail(AMSS_ERR_UNSUPPORTED, m.c_str());
+  }
   return 0;
 }
 
@@ -725,7 +620,7 @@ extern "C" int amss_engine_level_clock(amss_engine* e, int level, int* steps) {
 }
 
 extern "C" int amss_engine_set_level_clock(amss_engine* e, int level, int steps) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
   auto it = e->levels.find(level);
   if (it == e->levels.end() || steps < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_clock: bad level or steps");
   AMSS_CK(cudaStreamSynchronize(e->stream));
@@ -743,8 +638,9 @@ extern "C" int amss_engine_state_device(amss_engine* e, int block, double** dptr
 }
 
 extern "C" int amss_engine_enforce(amss_engine* e) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
   for (auto& b : e->blocks) {
+    if (b.owner != e->rank) continue;
     double* u = cur_state(e, b);
     AMSS_CK(launch_enforce(b.npts, b.fs, u + F_GXX * b.fs, u + F_AXX * b.fs, e->stream));
     e->launches++;
@@ -752,13 +648,7 @@ extern "C" int amss_engine_enforce(amss_engine* e) {
   return 0;
 }
 
-static int sync_level(amss_engine* e, ELevel& L, int which) {
-  if (L.sync.ntiles == 0) return 0;
-  AMSS_CK(launch_amr_sync(e->dblocks, L.sync.boxes, L.sync.tiles, L.sync.ntiles, which, e->prm.precision == 1,
-                          e->dstatus, e->stream));
-  e->launches++;
-  return 0;
-}
+static int sync_level(amss_engine* e, ELevel& L, int which) { return run_xfer(e, L.xsync, which); }
 
 // One RK4 step of every block of a level (bssn_class::Step, bssn_class.C:2981-3915):
 // four fused substep launches, a ghost sync after each, the ring rotation.
@@ -773,15 +663,24 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
   rk.chitiny = e->prm.chitiny;
   const bool mixed = e->prm.precision == 1;
   const int grid = std::min(L.ntiles, e->sm_count * 8);
+  // a rank without blocks on this level still takes part in its transfers
+  const bool work = !L.own.empty();
   // enforce_ga on U0 in place (bssn_class.C:3052); the stage outputs of
   // substeps 0-2 are enforced as they are written, which equals the
   // reference's in-place enforce_ga at the start of substeps 1-3 (:3416)
-  AMSS_CK(launch_amr_enforce(e->dblocks, L.dti_tiles, L.nti, e->stream));
-  e->launches++;
+  if (work) {
+    AMSS_CK(launch_amr_enforce(e->dblocks, L.dti_tiles, L.nti, e->stream));
+    e->launches++;
+  }
   const bool split = e->prm.kernel == 0;
   const int dgrid = std::min(L.nditems, e->sm_count * 16);
   const bool track = e->ntrack > 0 && level == e->track_level;
   for (int sub = 0; sub < 4; ++sub) {
+    if (!work) {
+      if (sub < 3)
+        if (int rc = sync_level(e, L, sub == 1 ? BUF_STAGE_B : BUF_STAGE_A)) return rc;
+      continue;
+    }
     cudaError_t err;
     const int enf = sub < 3 ? 1 : 0;
     if (track) {   // the substep's input state is complete (U0, or the synced stage)
@@ -838,17 +737,9 @@ static int restrict_prolong(amss_engine* e, int l, bool same_time) {
     e->launches++;
   }
   const int to_temp = same_time ? 0 : 1;
-  if (F.restrict_.ntiles) {
-    AMSS_CK(launch_amr_restrict(e->dblocks, F.restrict_.boxes, F.restrict_.tiles, F.restrict_.ntiles, to_temp,
-                                e->dstatus, e->stream));
-    e->launches++;
-  }
+  if (int rc = run_xfer(e, F.xrestrict, to_temp)) return rc;
   if (int rc = sync_level(e, C, same_time ? BUF_STATE : BUF_TEMP)) return rc;
-  if (F.prolong.ntiles) {
-    AMSS_CK(launch_amr_prolong(e->dblocks, F.prolong.boxes, F.prolong.tiles, F.prolong.ntiles, to_temp,
-                               e->dstatus, e->stream));
-    e->launches++;
-  }
+  if (int rc = run_xfer(e, F.xprolong, to_temp)) return rc;
   return sync_level(e, F, BUF_STATE);
 }
 
@@ -871,8 +762,8 @@ static int recursive_step(amss_engine* e, int l, double dt0) {
 
 template <typename T>
 static int patch_table_dw(amss_engine* e, ELevel& L) {
-  for (size_t m = 0; m < L.blocks.size(); ++m) {
-    const int dw = level_tile_w(L, e->blocks[L.blocks[m]].ex[0]);
+  for (size_t m = 0; m < L.own.size(); ++m) {
+    const int dw = level_tile_w(L, e->blocks[L.own[m]].ex[0]);
     char* dst = (char*)L.dtable + m * sizeof(StepBlock<T>) + offsetof(StepBlock<T>, dw);
     AMSS_CK(cudaMemcpy(dst, &dw, sizeof(int), cudaMemcpyHostToDevice));
   }
@@ -880,7 +771,7 @@ static int patch_table_dw(amss_engine* e, ELevel& L) {
 }
 
 extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_w, int zsplit) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_tiling: no such level");
   if (tile_w != 0 && (tile_w < kDerivMinEx || tile_w > DWMAX))
@@ -893,9 +784,10 @@ extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_
   const std::vector<DerivItem> items = deriv_items(e, L);
   if (L.ditems) cudaFree(L.ditems);
   L.ditems = nullptr;
+  L.nditems = (int)items.size();
+  if (items.empty()) return 0;
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
-  L.nditems = (int)items.size();
   return e->prm.precision == 1 ? patch_table_dw<float>(e, L) : patch_table_dw<double>(e, L);
 }
 
@@ -941,6 +833,8 @@ static AmrBlock amr_view(const amss_engine* e, const EBlock& b, int cur, int bac
 
 extern "C" int amss_engine_regrid_fill(amss_engine* dst, amss_engine* src, int level, int back) {
   if (!dst || !src || !dst->committed || !src->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (int rc = check_whole(dst, "amss_engine_regrid_fill")) return rc;
+  if (int rc = check_whole(src, "amss_engine_regrid_fill")) return rc;
   if (dst == src) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: source and destination are one engine");
   if (back != 0 && back != 1) return amss_fail(AMSS_ERR_ARG, "amss_engine_regrid_fill: back must be 0 or 1");
   if (dst->nf != src->nf || dst->prm.precision != src->prm.precision)
@@ -1024,12 +918,14 @@ extern "C" int amss_engine_regrid_fill(amss_engine* dst, amss_engine* src, int l
 }
 
 extern "C" int amss_engine_step_level(amss_engine* e, int level, double dt) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (e->nranks > 1) AMSS_CK(cudaSetDevice(e->device));   // each rank's thread drives its own GPU
   return step_level_impl(e, level, dt);
 }
 
 extern "C" int amss_engine_coarse_step(amss_engine* e, double dt0) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (e->nranks > 1) AMSS_CK(cudaSetDevice(e->device));   // each rank's thread drives its own GPU
   return recursive_step(e, 0, dt0);
 }
 
@@ -1079,18 +975,19 @@ static int run_graph(amss_engine* e, int level, double dt, int nsteps, int repla
 }
 
 extern "C" int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int replays) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (int rc = check_whole(e, "amss_engine_run_graph")) return rc;
   if (level < 0) return amss_fail(AMSS_ERR_ARG, "amss_engine_run_graph: level must be >= 0");
   return run_graph(e, level, dt, nsteps, replays);
 }
 
 extern "C" int amss_engine_run_coarse_graph(amss_engine* e, double dt0, int nsteps, int replays) {
-  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  if (int rc = check_whole(e, "amss_engine_run_coarse_graph")) return rc;
   return run_graph(e, -1, dt0, nsteps, replays);
 }
 
 extern "C" int amss_engine_sync(amss_engine* e) {
   if (!e) return AMSS_ERR_ARG;
+  if (e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_sync: a plan has no device state");
   AMSS_CK(cudaStreamSynchronize(e->stream));
   unsigned st = 0;
   AMSS_CK(cudaMemcpy(&st, e->dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost));
@@ -1107,16 +1004,20 @@ extern "C" long long amss_engine_level_points(amss_engine* e, int level) {
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return 0;
   long long n = 0;
-  for (int b : it->second.blocks) n += e->blocks[b].npts;
+  for (int b : it->second.own) n += e->blocks[b].npts;
   return n;
 }
 
-extern "C" int amss_engine_constraint_norms(amss_engine* e, int level, double* norms) {
-  if (!e || !norms) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms: null argument");
-  if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_constraint_norms: commit the engine first");
+extern "C" int amss_engine_constraint_sums(amss_engine* e, int level, double* sums) {
+  if (!e || !sums) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_sums: null argument");
+  if (!e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_constraint_sums: commit the engine first");
   auto it = e->levels.find(level);
-  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms: no such level");
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_sums: no such level");
   ELevel& L = it->second;
+  if (L.own.empty()) {   // a rank without blocks on the level adds nothing
+    for (int c = 0; c < 8; ++c) sums[c] = 0.0;
+    return 0;
+  }
   constexpr int kGrid = 148 * 2;
   if (e->cons_cap < 7 * L.dfs) {
     if (e->cons) cudaFree(e->cons);
@@ -1141,8 +1042,16 @@ extern "C" int amss_engine_constraint_norms(amss_engine* e, int level, double* n
   for (int c = 0; c < 8; ++c) {
     double v = 0.0;
     for (int g = 0; g < kGrid; ++g) v += part[(size_t)g * 8 + c];   // fixed order: reproducible
-    norms[c] = std::sqrt(v);
+    sums[c] = v;
   }
+  return 0;
+}
+
+extern "C" int amss_engine_constraint_norms(amss_engine* e, int level, double* norms) {
+  if (!norms) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms: null argument");
+  double s[8];
+  if (int rc = amss_engine_constraint_sums(e, level, s)) return rc;
+  for (int c = 0; c < 8; ++c) norms[c] = std::sqrt(s[c]);
   return 0;
 }
 
@@ -1210,6 +1119,7 @@ extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, co
   if (!e || (npts > 0 && (!xyz || !out)) || nvar < 1 || !fields)
     return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: null argument or nvar < 1");
   if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_interp_points: commit the engine first");
+  if (int rc = check_whole(e, "amss_engine_interp_points")) return rc;
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: no such level");
   for (int v = 0; v < nvar; ++v)
@@ -1300,6 +1210,7 @@ extern "C" int amss_engine_set_punctures(amss_engine* e, int n, const double* po
   if (!e || n < 0 || n > kMaxPunctures || (n > 0 && !pos))
     return amss_fail(AMSS_ERR_ARG, "amss_engine_set_punctures: 0 <= n <= 10 positions");
   if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_set_punctures: commit the engine first");
+  if (int rc = check_whole(e, "amss_engine_set_punctures")) return rc;
   e->ntrack = 0;
   if (n == 0) return 0;
   const int level = e->levels.rbegin()->first;
