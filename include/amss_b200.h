@@ -356,6 +356,29 @@ int amss_engine_set_punctures(amss_engine* e, int n, const double* pos);
  * for the engine's stream. */
 int amss_engine_get_punctures(amss_engine* e, double* pos);
 
+/* ---- Wave extraction (bssn_class::AnalysisStuff, bssn_class.C:6945-7285).
+ *
+ * amss_engine_psi4: bssn_class::Compute_Psi4 (bssn_class.C:6210-6298) with
+ * getnp4 (getnp4.f90:12-452; Psi4type 0, tetradtype 2): the Newman-Penrose
+ * scalar Psi4 of the level's current state on every point of its blocks,
+ * then the level's ghost sync.  The Christoffel symbols and Ricci tensor it
+ * needs are those of the same state (the reference reuses the last
+ * compute_rhs_bssn outputs of the level).  The result lives in each block's
+ * RK4 accumulator, fields 0 (Rpsi4) and 1 (Ipsi4), until the next step;
+ * amss_engine_get_psi4 copies a block's two fields to the host (2 x npts).
+ * BSSN engines only.
+ *
+ * amss_engine_psi4_modes: surface_integral::surf_Wave (surface_integral.C:
+ * 197-377 with GaussInt; its sphere, :39-181): Psi4 interpolated on the
+ * sphere of radius rex (N_theta = 2 nquarter Gauss-Legendre nodes in
+ * cos(theta), N_phi = 4 nquarter midpoints in phi, reduced per symmetry) and
+ * projected on the spin-weight -2 harmonics: RP, IP get (maxl+1)^2 - 4 values,
+ * l = 2..maxl, m = -l..l, the bssn_psi4.dat columns.  Every sphere point must
+ * lie in the level's patches (AMSS_ERR_ARG otherwise). */
+int amss_engine_psi4(amss_engine* e, int level);
+int amss_engine_get_psi4(amss_engine* e, int block, double* host);
+int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int nquarter, int maxl, double* RP, double* IP);
+
 /* ---- Blocks divided among ranks, one engine per GPU (Parallel::distribute,
  * Parallel.C:504-827, assigns the reference's blocks to MPI ranks;
  * Parallel::Sync / transfer, Parallel.C:3677-3776 and :3508-3592, move the

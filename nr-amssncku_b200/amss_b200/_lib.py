@@ -105,6 +105,10 @@ def lib():
     L.amss_engine_xfer_peers.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     L.amss_engine_staging_block.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    L.amss_engine_psi4.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.amss_engine_get_psi4.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+    L.amss_engine_psi4_modes.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         _DP, _DP]
     _lib = L
     return L
 

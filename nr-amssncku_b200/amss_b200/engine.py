@@ -208,6 +208,28 @@ class Engine:
               "amss_engine_constraint_sums")
         return out
 
+    def psi4(self, level):
+        """Psi4 of a level's current state (bssn_class::Compute_Psi4 with
+        getnp4), kept on the device until the next step."""
+        check(lib().amss_engine_psi4(self._h, level), "amss_engine_psi4")
+
+    def get_psi4(self, block):
+        """(Rpsi4, Ipsi4) of one block after psi4(): (2, ez, ey, ex)."""
+        ex = self.blocks[block]
+        out = np.empty((2, ex[2], ex[1], ex[0]))
+        check(lib().amss_engine_get_psi4(self._h, block, out.ctypes.data_as(_DP)), "amss_engine_get_psi4")
+        return out
+
+    def psi4_modes(self, level, rex, nquarter=40, maxl=8):
+        """surface_integral::surf_Wave after psi4(): the spin-weight -2 modes
+        (l = 2..maxl, m = -l..l) of Psi4 on the sphere of radius rex, as two
+        arrays (RP, IP)."""
+        nn = (maxl + 1) ** 2 - 4
+        rp, ip = np.zeros(nn), np.zeros(nn)
+        check(lib().amss_engine_psi4_modes(self._h, level, float(rex), int(nquarter), int(maxl),
+                                           rp.ctypes.data_as(_DP), ip.ctypes.data_as(_DP)), "amss_engine_psi4_modes")
+        return rp, ip
+
     def interp_points(self, level, points, fields, soa=None):
         """Values of state fields at points of a level (Parallel::PatList_Interp_Points,
         Parallel.C:5614-5667): points (n, 3), fields a list of state indices,

@@ -1,5 +1,5 @@
-"""The constraint output file of an evolution (bssn_constraint.dat), written
-from the engine's constraint monitor.
+"""The analysis output files of an evolution: bssn_constraint.dat from the
+engine's constraint monitor, and bssn_psi4.dat from its wave extraction.
 
 File format and cadence follow the reference:
 
@@ -17,6 +17,11 @@ File format and cadence follow the reference:
   AnasTime, one line per level (levels in order, all at the same PhysTime) with
   the 7 norms of Parallel::L2Norm, and LastConsOut goes back to 0.  A Z4c run
   writes 8 values per line, Theta's norm last (Z4c_class.C:2502-2511).
+* bssn_psi4.dat (bssn_class.C:76-88 header, :7143-7263 AnalysisStuff): the
+  column header names R{l:02d}m{m:03d} and I{l:02d}m{m:03d} for l = 2..maxl,
+  m = -l..l, each in a field of 16 after "# time" in a field of 15; one line
+  per detector radius (maxrex, maxrex - drex, ...) with the time and the
+  (RP, IP) pairs (monitor::writefile with two arrays, monitor.C:151-165).
 """
 import os
 import time
@@ -68,6 +73,56 @@ class ConstraintMonitor:
         self.last += dT * 0.5 ** max(0, self.trfls)
         if self.last >= self.anas_time:
             self.write(engine, phys_time, nlevels)
+            self.last = 0.0
+            return True
+        return False
+
+
+def psi4_header(maxl):
+    """bssn_class.C:76-88: the column header of bssn_psi4.dat."""
+    s = "%-15s" % "# time"
+    for l in range(2, maxl + 1):
+        for m in range(-l, l + 1):
+            s += "%-16s" % ("R%02dm%03d" % (l, m)) + "%-16s" % ("I%02dm%03d" % (l, m))
+    return s
+
+
+class WaveMonitor:
+    """bssn_psi4.dat for an engine: at each analysis time, Psi4 of level
+    `level` and its modes on decn spheres of radius maxrex, maxrex - drex, ...
+    (AnalysisStuff, bssn_class.C:6945-7285, every AnasTime of the analysis
+    level's clock)."""
+
+    def __init__(self, out_dir, anas_time, level, maxl=8, decn=1, maxrex=None, drex=0.0, nquarter=40,
+                 name="bssn_psi4.dat"):
+        if maxrex is None:
+            raise ValueError("WaveMonitor: maxrex (the outermost extraction radius) is required")
+        self.path = open_name(out_dir, name)
+        self.anas_time = float(anas_time)
+        self.level, self.maxl, self.decn = int(level), int(maxl), int(decn)
+        self.maxrex, self.drex, self.nquarter = float(maxrex), float(drex), int(nquarter)
+        self.last = 0.0   # LastAnas
+        with open(self.path, "w") as f:
+            f.write("# File created on " + time.asctime() + "\n")
+            f.write("#\n")
+            f.write(psi4_header(self.maxl) + "\n")
+
+    def write(self, engine, phys_time):
+        engine.psi4(self.level)
+        rex = self.maxrex
+        with open(self.path, "a") as f:
+            for _ in range(self.decn):
+                rp, ip = engine.psi4_modes(self.level, rex, self.nquarter, self.maxl)
+                vals = [v for pair in zip(rp, ip) for v in pair]
+                f.write(format_line(phys_time, vals) + "\n")
+                rex -= self.drex
+
+    def after_step(self, engine, phys_time, dT_lev):
+        """AnalysisStuff's clock: LastAnas += dT_lev; write when it reaches
+        AnasTime.  Returns True when it wrote."""
+        self.last += dT_lev
+        if self.last >= self.anas_time:
+            self.write(engine, phys_time)
             self.last = 0.0
             return True
         return False

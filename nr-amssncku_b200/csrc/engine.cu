@@ -53,6 +53,11 @@ cudaError_t launch_amr_restrict(const AmrBlock* blocks, const AmrBox* boxes, con
 cudaError_t launch_amr_timeinterp(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
 cudaError_t launch_amr_rotate(int* lvl, cudaStream_t s);
 cudaError_t launch_amr_enforce(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
+template <typename T>
+cudaError_t launch_psi4(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm, double* scratch,
+                        long long dfs, cudaStream_t s);
+void gauss_legendre_desc(int n, std::vector<double>& x, std::vector<double>& w);
+double wigner_d(int l, int m, int s, double costheta);
 
 static thread_local std::string g_err;
 
@@ -132,6 +137,7 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
   if (e->dstatus) cudaFree(e->dstatus);
   if (e->cons) cudaFree(e->cons);
   if (e->cpart) cudaFree(e->cpart);
+  if (e->pscr) cudaFree(e->pscr);
   if (e->iitems) cudaFree(e->iitems);
   if (e->dtrack) cudaFree(e->dtrack);
   if (e->dtpatch) cudaFree(e->dtpatch);
@@ -1114,8 +1120,10 @@ static void find_box(const EBlock& b, const IPatch& q, double lo[3], double hi[3
 // a side it shares with the patch box) holds it to half a cell; and the
 // stencil choice of global_interp (fmisc.f90:738-781, ORDN = 6).  Blocks added
 // by bbox form one patch per distinct patch box, with no buffer.
-extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, const double* xyz, int nvar,
-                                         const int* fields, const double* soa, double* out, int* found) {
+// from_acc: the fields are those of the blocks' accumulators K (Psi4 after
+// amss_engine_psi4) instead of the current state.
+static int interp_level(amss_engine* e, int level, int npts, const double* xyz, int nvar, const int* fields,
+                        const double* soa, double* out, int* found, bool from_acc) {
   if (!e || (npts > 0 && (!xyz || !out)) || nvar < 1 || !fields)
     return amss_fail(AMSS_ERR_ARG, "amss_engine_interp_points: null argument or nvar < 1");
   if (!e->committed) return amss_fail(AMSS_ERR_STATE, "amss_engine_interp_points: commit the engine first");
@@ -1164,7 +1172,7 @@ extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, co
           t.cxB[d] = cxB;
           t.cx[d] = cxB > 0 ? (pt[d] - c[cxB - 1]) / dd : (pt[d] + c[-cxB]) / dd;
         }
-        const double* u = cur_state(e, b);
+        const double* u = from_acc ? b.K : cur_state(e, b);
         for (int v = 0; v < nvar; ++v) {
           t.f = u + (long long)fields[v] * b.fs;
           for (int d = 0; d < 3; ++d) t.soa[d] = soa ? soa[3 * v + d] : 1.0;
@@ -1200,6 +1208,128 @@ extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, co
   AMSS_CK(cudaMemcpyAsync(res.data(), e->iout, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
   AMSS_CK(cudaStreamSynchronize(e->stream));
   for (long long i = 0; i < n; ++i) out[where[i]] = res[i];
+  return 0;
+}
+
+extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, const double* xyz, int nvar,
+                                         const int* fields, const double* soa, double* out, int* found) {
+  return interp_level(e, level, npts, xyz, nvar, fields, soa, out, found, false);
+}
+
+// bssn_class::Compute_Psi4 (bssn_class.C:6210-6298): Psi4 of the level's
+// current state on every point of its blocks, then the level's ghost sync.
+extern "C" int amss_engine_psi4(amss_engine* e, int level) {
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_psi4: commit the engine first");
+  if (e->nf != NFIELDS_BSSN) return amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_psi4: BSSN engines only (getnp4)");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_psi4: no such level");
+  ELevel& L = it->second;
+  if (!L.own.empty()) {
+    if (e->pscr_cap < 24 * L.dfs) {
+      if (e->pscr) cudaFree(e->pscr);
+      e->pscr = nullptr;
+      e->pscr_cap = 0;
+      AMSS_CK(cudaMalloc(&e->pscr, (size_t)24 * L.dfs * sizeof(double)));
+      e->pscr_cap = 24 * L.dfs;
+    }
+    const int tile_pts = e->prm.kernel == 0 ? (int)kPointwiseTile : 128;
+    const cudaError_t err =
+        e->prm.precision == 1
+            ? launch_psi4<float>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, e->pscr, L.dfs, e->stream)
+            : launch_psi4<double>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, e->pscr, L.dfs, e->stream);
+    AMSS_CK(err);
+    e->launches += 2;
+  }
+  return run_xfer(e, L.xsync, BUF_TEMP);   // Parallel::Sync of Rpsi4 / Ipsi4
+}
+
+extern "C" int amss_engine_get_psi4(amss_engine* e, int block, double* h) {
+  if (int rc = check_block(e, block)) return rc;
+  if (!h) return amss_fail(AMSS_ERR_ARG, "amss_engine_get_psi4: null buffer");
+  EBlock& b = e->blocks[block];
+  AMSS_CK(cudaMemcpy2DAsync(h, b.npts * sizeof(double), b.K, b.fs * sizeof(double), b.npts * sizeof(double), 2,
+                            cudaMemcpyDeviceToHost, e->stream));
+  AMSS_CK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+// surface_integral::surf_Wave (surface_integral.C:197-377, GaussInt; sphere of
+// surface_integral.C:39-181): Psi4 of the level (amss_engine_psi4 first)
+// interpolated at N_theta x N_phi points of the sphere of radius rex --
+// Gauss-Legendre nodes in cos(theta) (the upper hemisphere first), midpoints
+// in phi, N_theta = 2N, N_phi = 4N, halved in theta for Symmetry 1 and also
+// quartered in phi for Symmetry 2 -- and projected on the spin-weight -2
+// harmonics, l = 2..maxl, m = -l..l; the mirrored parts of the sphere enter
+// through the parities of Rpsi4 (+, +, +) and Ipsi4 (-, -, -).
+extern "C" int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int nquarter, int maxl, double* RP,
+                                      double* IP) {
+  if (!RP || !IP || !(rex > 0) || nquarter < 1 || maxl < 2)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_psi4_modes: rex > 0, N >= 1, maxl >= 2 and output arrays");
+  if (int rc = check_whole(e, "amss_engine_psi4_modes")) return rc;
+  const int sym = e->prm.symmetry;
+  int n_phi = 4 * nquarter, n_theta = 2 * nquarter;
+  std::vector<double> ct, wt;
+  gauss_legendre_desc(n_theta, ct, wt);
+  double dphi;
+  if (sym == 2) {
+    n_phi /= 4;
+    n_theta /= 2;
+    dphi = M_PI / (2.0 * n_phi);
+  } else if (sym == 1) {
+    n_theta /= 2;
+    dphi = 2.0 * M_PI / n_phi;
+  } else {
+    dphi = 2.0 * M_PI / n_phi;
+  }
+  const int ntot = n_theta * n_phi;
+  std::vector<double> xyz(3 * (size_t)ntot);
+  for (int i = 0, n = 0; i < n_theta; ++i) {
+    const double s = std::sqrt(1.0 - ct[i] * ct[i]);
+    for (int j = 0; j < n_phi; ++j, ++n) {
+      const double ph = (j + 0.5) * dphi;
+      xyz[3 * n] = rex * (s * std::cos(ph));
+      xyz[3 * n + 1] = rex * (s * std::sin(ph));
+      xyz[3 * n + 2] = rex * ct[i];
+    }
+  }
+  const int fields[2] = {0, 1};
+  const double soa[6] = {1, 1, 1, -1, -1, -1};   // Rpsi4, Ipsi4 (bssn_class.C:347-348)
+  std::vector<double> v(2 * (size_t)ntot);
+  std::vector<int> found(ntot);
+  if (int rc = interp_level(e, level, ntot, xyz.data(), 2, fields, soa, v.data(), found.data(), true)) return rc;
+  for (int n = 0; n < ntot; ++n)
+    if (!found[n]) return amss_fail(AMSS_ERR_ARG, "amss_engine_psi4_modes: the sphere leaves the level's patches");
+  const int nn = (maxl + 1) * (maxl + 1) - 4;
+  std::vector<double> rp(nn, 0.0), ip(nn, 0.0);
+  const int lpsy = sym == 0 ? 1 : (sym == 1 ? 2 : 8);
+  // per mirror image lp: the sign of cos(theta), the phi map, the parity factors
+  for (int n = 0; n < ntot; ++n) {
+    const int i = n / n_phi, j = n - i * n_phi;
+    const double R = v[2 * n], I = v[2 * n + 1];
+    int c = 0;
+    for (int l = 2; l <= maxl; ++l)
+      for (int m = -l; m <= l; ++m, ++c)
+        for (int lp = 0; lp < lpsy; ++lp) {
+          const bool flip_z = lp & 1, flip_y = (lp == 2 || lp == 3 || lp == 6 || lp == 7), flip_x = lp >= 4;
+          const double cth = flip_z ? -ct[i] : ct[i];
+          double arg;
+          if (lp < 4) arg = m * (j + 0.5) * dphi;
+          else if (lp < 6) arg = m * (M_PI - (j + 0.5) * dphi);
+          else arg = m * (M_PI + (j + 0.5) * dphi);
+          const double cm = std::cos(arg);
+          const double sm = (lp == 2 || lp == 3) ? -std::sin(arg) : std::sin(arg);
+          // Rpsi4 is even in every direction; Ipsi4 odd in each flipped one
+          const double sI = ((flip_x ? -1.0 : 1.0) * (flip_y ? -1.0 : 1.0)) * (flip_z ? -1.0 : 1.0);
+          const double r = R, im = sI * I;
+          const double th = std::sqrt((2 * l + 1.0) / 4.0 / M_PI) * wigner_d(l, m, 2, cth);
+          rp[c] = rp[c] + th * (r * cm + im * sm) * wt[i];
+          ip[c] = ip[c] + th * (im * cm - r * sm) * wt[i];
+        }
+  }
+  for (int c = 0; c < nn; ++c) {
+    RP[c] = rp[c] * rex * dphi;
+    IP[c] = ip[c] * rex * dphi;
+  }
   return 0;
 }
 

@@ -154,6 +154,8 @@ struct amss_engine {
   double* cons = nullptr;       // constraint residuals of a level (7 x its D stride), grow-only
   long long cons_cap = 0;
   double* cpart = nullptr;      // per-CTA partial sums of the constraint norms (8 each)
+  double* pscr = nullptr;       // Christoffel symbols and Ricci tensor of a level for Psi4 (24 x its D stride), grow-only
+  long long pscr_cap = 0;
   int ntrack = 0, track_level = -1;   // puncture tracking on the finest level
   amss::TrackState* dtrack = nullptr;
   amss::TrackPatch* dtpatch = nullptr;
