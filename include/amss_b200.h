@@ -379,6 +379,15 @@ int amss_engine_psi4(amss_engine* e, int level);
 int amss_engine_get_psi4(amss_engine* e, int block, double* host);
 int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int nquarter, int maxl, double* RP, double* IP);
 
+/* surface_integral::surf_MassPAng (surface_integral.C:2247-2512, GaussInt,
+ * with admmass_bssn, fadmquantites_bssn.f90:5-65): the ADM mass, linear
+ * momentum and angular momentum through the sphere of radius rex of the same
+ * quadrature, from the level's current state.  out[7]: mass, Px, Py, Pz, Sx,
+ * Sy, Sz, the bssn_ADMQs.dat columns (Symmetry 1 gives only Px, Py, Sz of the
+ * momenta, Symmetry 2 none; the others are 0).  Overwrites accumulator
+ * fields 2-4 (Psi4 in fields 0, 1 stays).  BSSN engines only. */
+int amss_engine_adm_integrals(amss_engine* e, int level, double rex, int nquarter, double out[7]);
+
 /* ---- Blocks divided among ranks, one engine per GPU (Parallel::distribute,
  * Parallel.C:504-827, assigns the reference's blocks to MPI ranks;
  * Parallel::Sync / transfer, Parallel.C:3677-3776 and :3508-3592, move the

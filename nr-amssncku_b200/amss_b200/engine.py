@@ -230,6 +230,14 @@ class Engine:
                                            rp.ctypes.data_as(_DP), ip.ctypes.data_as(_DP)), "amss_engine_psi4_modes")
         return rp, ip
 
+    def adm_integrals(self, level, rex, nquarter=40):
+        """surface_integral::surf_MassPAng: (mass, Px, Py, Pz, Sx, Sy, Sz)
+        through the sphere of radius rex on a level."""
+        out = np.zeros(7)
+        check(lib().amss_engine_adm_integrals(self._h, level, float(rex), int(nquarter), out.ctypes.data_as(_DP)),
+              "amss_engine_adm_integrals")
+        return out
+
     def interp_points(self, level, points, fields, soa=None):
         """Values of state fields at points of a level (Parallel::PatList_Interp_Points,
         Parallel.C:5614-5667): points (n, 3), fields a list of state indices,

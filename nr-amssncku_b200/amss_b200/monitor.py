@@ -21,7 +21,8 @@ File format and cadence follow the reference:
   column header names R{l:02d}m{m:03d} and I{l:02d}m{m:03d} for l = 2..maxl,
   m = -l..l, each in a field of 16 after "# time" in a field of 15; one line
   per detector radius (maxrex, maxrex - drex, ...) with the time and the
-  (RP, IP) pairs (monitor::writefile with two arrays, monitor.C:151-165).
+  (RP, IP) pairs (monitor::writefile with two arrays, monitor.C:151-165);
+  bssn_ADMQs.dat the same lines with the 7 ADM integrals of surf_MassPAng.
 """
 import os
 import time
@@ -87,34 +88,41 @@ def psi4_header(maxl):
     return s
 
 
+ADM_HEADER = "%-15s" % "# time ADMmass ADMPx ADMPy ADMPz ADMSx ADMSy ADMSz"   # bssn_class.C:95-98
+
+
 class WaveMonitor:
-    """bssn_psi4.dat for an engine: at each analysis time, Psi4 of level
-    `level` and its modes on decn spheres of radius maxrex, maxrex - drex, ...
+    """bssn_psi4.dat and bssn_ADMQs.dat for an engine: at each analysis
+    time, Psi4 of level `level` and its modes, and the ADM mass, momentum and
+    angular momentum, on decn spheres of radius maxrex, maxrex - drex, ...
     (AnalysisStuff, bssn_class.C:6945-7285, every AnasTime of the analysis
     level's clock)."""
 
     def __init__(self, out_dir, anas_time, level, maxl=8, decn=1, maxrex=None, drex=0.0, nquarter=40,
-                 name="bssn_psi4.dat"):
+                 name="bssn_psi4.dat", adm_name="bssn_ADMQs.dat"):
         if maxrex is None:
             raise ValueError("WaveMonitor: maxrex (the outermost extraction radius) is required")
         self.path = open_name(out_dir, name)
+        self.adm_path = open_name(out_dir, adm_name)
         self.anas_time = float(anas_time)
         self.level, self.maxl, self.decn = int(level), int(maxl), int(decn)
         self.maxrex, self.drex, self.nquarter = float(maxrex), float(drex), int(nquarter)
         self.last = 0.0   # LastAnas
-        with open(self.path, "w") as f:
-            f.write("# File created on " + time.asctime() + "\n")
-            f.write("#\n")
-            f.write(psi4_header(self.maxl) + "\n")
+        for path, head in ((self.path, psi4_header(self.maxl)), (self.adm_path, ADM_HEADER)):
+            with open(path, "w") as f:
+                f.write("# File created on " + time.asctime() + "\n")
+                f.write("#\n")
+                f.write(head + "\n")
 
     def write(self, engine, phys_time):
         engine.psi4(self.level)
         rex = self.maxrex
-        with open(self.path, "a") as f:
+        with open(self.path, "a") as f, open(self.adm_path, "a") as g:
             for _ in range(self.decn):
                 rp, ip = engine.psi4_modes(self.level, rex, self.nquarter, self.maxl)
                 vals = [v for pair in zip(rp, ip) for v in pair]
                 f.write(format_line(phys_time, vals) + "\n")
+                g.write(format_line(phys_time, engine.adm_integrals(self.level, rex, self.nquarter)) + "\n")
                 rex -= self.drex
 
     def after_step(self, engine, phys_time, dT_lev):

@@ -56,6 +56,8 @@ cudaError_t launch_amr_enforce(const AmrBlock* blocks, const int2* tiles, int nt
 template <typename T>
 cudaError_t launch_psi4(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm, double* scratch,
                         long long dfs, cudaStream_t s);
+template <typename T>
+cudaError_t launch_admmass(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm, cudaStream_t s);
 void gauss_legendre_desc(int n, std::vector<double>& x, std::vector<double>& w);
 double wigner_d(int l, int m, int s, double costheta);
 
@@ -1253,6 +1255,53 @@ extern "C" int amss_engine_get_psi4(amss_engine* e, int block, double* h) {
   return 0;
 }
 
+// The sphere of surface_integral::surface_integral (surface_integral.C:39-181,
+// GaussInt): N_theta = 2N Gauss-Legendre nodes in cos(theta), upper
+// hemisphere first, N_phi = 4N midpoints in phi; Symmetry 1 keeps the upper
+// half, Symmetry 2 also a quarter in phi (factor: the copies it stands for).
+struct Sphere {
+  int n_theta, n_phi, ntot, factor;
+  double dphi;
+  std::vector<double> ct, wt, nx, ny, nz, xyz;
+};
+static Sphere make_sphere(int nquarter, int sym, double rex) {
+  Sphere S;
+  S.n_phi = 4 * nquarter;
+  S.n_theta = 2 * nquarter;
+  gauss_legendre_desc(S.n_theta, S.ct, S.wt);
+  if (sym == 2) {
+    S.n_phi /= 4;
+    S.n_theta /= 2;
+    S.dphi = M_PI / (2.0 * S.n_phi);
+    S.factor = 8;
+  } else if (sym == 1) {
+    S.n_theta /= 2;
+    S.dphi = 2.0 * M_PI / S.n_phi;
+    S.factor = 2;
+  } else {
+    S.dphi = 2.0 * M_PI / S.n_phi;
+    S.factor = 1;
+  }
+  S.ntot = S.n_theta * S.n_phi;
+  S.xyz.resize(3 * (size_t)S.ntot);
+  S.nx.resize(S.ntot);
+  S.ny.resize(S.ntot);
+  S.nz.resize(S.ntot);
+  for (int i = 0, n = 0; i < S.n_theta; ++i) {
+    const double s = std::sqrt(1.0 - S.ct[i] * S.ct[i]);
+    for (int j = 0; j < S.n_phi; ++j, ++n) {
+      const double ph = (j + 0.5) * S.dphi;
+      S.nx[n] = s * std::cos(ph);
+      S.ny[n] = s * std::sin(ph);
+      S.nz[n] = S.ct[i];
+      S.xyz[3 * n] = rex * S.nx[n];
+      S.xyz[3 * n + 1] = rex * S.ny[n];
+      S.xyz[3 * n + 2] = rex * S.nz[n];
+    }
+  }
+  return S;
+}
+
 // surface_integral::surf_Wave (surface_integral.C:197-377, GaussInt; sphere of
 // surface_integral.C:39-181): Psi4 of the level (amss_engine_psi4 first)
 // interpolated at N_theta x N_phi points of the sphere of radius rex --
@@ -1267,31 +1316,12 @@ extern "C" int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int
     return amss_fail(AMSS_ERR_ARG, "amss_engine_psi4_modes: rex > 0, N >= 1, maxl >= 2 and output arrays");
   if (int rc = check_whole(e, "amss_engine_psi4_modes")) return rc;
   const int sym = e->prm.symmetry;
-  int n_phi = 4 * nquarter, n_theta = 2 * nquarter;
-  std::vector<double> ct, wt;
-  gauss_legendre_desc(n_theta, ct, wt);
-  double dphi;
-  if (sym == 2) {
-    n_phi /= 4;
-    n_theta /= 2;
-    dphi = M_PI / (2.0 * n_phi);
-  } else if (sym == 1) {
-    n_theta /= 2;
-    dphi = 2.0 * M_PI / n_phi;
-  } else {
-    dphi = 2.0 * M_PI / n_phi;
-  }
-  const int ntot = n_theta * n_phi;
-  std::vector<double> xyz(3 * (size_t)ntot);
-  for (int i = 0, n = 0; i < n_theta; ++i) {
-    const double s = std::sqrt(1.0 - ct[i] * ct[i]);
-    for (int j = 0; j < n_phi; ++j, ++n) {
-      const double ph = (j + 0.5) * dphi;
-      xyz[3 * n] = rex * (s * std::cos(ph));
-      xyz[3 * n + 1] = rex * (s * std::sin(ph));
-      xyz[3 * n + 2] = rex * ct[i];
-    }
-  }
+  const Sphere S = make_sphere(nquarter, sym, rex);
+  const int n_phi = S.n_phi, ntot = S.ntot;
+  const double dphi = S.dphi;
+  const std::vector<double>& ct = S.ct;
+  const std::vector<double>& wt = S.wt;
+  const std::vector<double>& xyz = S.xyz;
   const int fields[2] = {0, 1};
   const double soa[6] = {1, 1, 1, -1, -1, -1};   // Rpsi4, Ipsi4 (bssn_class.C:347-348)
   std::vector<double> v(2 * (size_t)ntot);
@@ -1330,6 +1360,108 @@ extern "C" int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int
     RP[c] = rp[c] * rex * dphi;
     IP[c] = ip[c] * rex * dphi;
   }
+  return 0;
+}
+
+// surface_integral::surf_MassPAng (surface_integral.C:2247-2512, GaussInt):
+// the ADM mass, linear and angular momentum through the sphere of radius rex
+// on a level.  The mass integrand of admmass_bssn is formed on the level's
+// blocks (accumulator fields 2-4, not synchronised, as the reference leaves
+// its temporaries), interpolated with chi, trK, the metric and A~ij at the
+// sphere's points, and summed with the Gauss-Legendre weights.  Symmetry 1
+// integrates S_z, P_x and P_y only, Symmetry 2 the mass only (the others 0).
+// out: mass, Px, Py, Pz, Sx, Sy, Sz (the bssn_ADMQs.dat columns).
+extern "C" int amss_engine_adm_integrals(amss_engine* e, int level, double rex, int nquarter, double* out) {
+  if (!out || !(rex > 0) || nquarter < 1)
+    return amss_fail(AMSS_ERR_ARG, "amss_engine_adm_integrals: rex > 0, N >= 1 and an output array");
+  if (int rc = check_whole(e, "amss_engine_adm_integrals")) return rc;
+  if (e->nf != NFIELDS_BSSN) return amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_adm_integrals: BSSN engines only");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_adm_integrals: no such level");
+  ELevel& L = it->second;
+  const int tile_pts = e->prm.kernel == 0 ? (int)kPointwiseTile : 128;
+  AMSS_CK(e->prm.precision == 1 ? launch_admmass<float>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, e->stream)
+                                : launch_admmass<double>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, e->stream));
+  e->launches++;
+  const int sym = e->prm.symmetry;
+  const Sphere S = make_sphere(nquarter, sym, rex);
+  const int ntot = S.ntot;
+  // the mass integrand has the shift's parities; chi .. A~zz the state's
+  const int mfields[3] = {2, 3, 4};
+  const double msoa[9] = {-1, 1, 1, 1, -1, 1, 1, 1, -1};
+  const int sfields[14] = {F_CHI, F_TRK, F_GXX, F_GXY, F_GXZ, F_GYY, F_GYZ, F_GZZ,
+                           F_AXX, F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ};
+  double ssoa[42];
+  for (int v = 0; v < 14; ++v)
+    for (int d = 0; d < 3; ++d) ssoa[3 * v + d] = soa_sign(sfields[v], d);
+  std::vector<double> mv(3 * (size_t)ntot), sv(14 * (size_t)ntot);
+  std::vector<int> found(ntot);
+  if (int rc = interp_level(e, level, ntot, S.xyz.data(), 3, mfields, msoa, mv.data(), found.data(), true)) return rc;
+  for (int n = 0; n < ntot; ++n)
+    if (!found[n]) return amss_fail(AMSS_ERR_ARG, "amss_engine_adm_integrals: the sphere leaves the level's patches");
+  if (int rc = interp_level(e, level, ntot, S.xyz.data(), 14, sfields, ssoa, sv.data(), nullptr, false)) return rc;
+  const double f1o8 = 0.125;
+  double mass = 0, sx = 0, sy = 0, sz = 0, px = 0, py = 0, pz = 0;
+  for (int n = 0; n < ntot; ++n) {
+    const int i = n / S.n_phi;
+    const double* m = &mv[3 * (size_t)n];
+    const double* s = &sv[14 * (size_t)n];
+    const double nx = S.nx[n], ny = S.ny[n], nz = S.nz[n], w = S.wt[i];
+    const double X = S.xyz[3 * n], Y = S.xyz[3 * n + 1], Z = S.xyz[3 * n + 2];
+    double Chi = s[0];
+    const double TRK = s[1];
+    const double Gxx = s[2] + 1.0, Gxy = s[3], Gxz = s[4], Gyy = s[5] + 1.0, Gyz = s[6], Gzz = s[7] + 1.0;
+    double axx = s[8], axy = s[9], axz = s[10], ayy = s[11], ayz = s[12], azz = s[13];
+    Chi = 1.0 / (1.0 + Chi);          // psi^4
+    const double Psi = Chi * std::sqrt(Chi);   // psi^6
+    mass = mass + (m[0] * nx + m[1] * ny + m[2] * nz) * w;
+    double gupzz = Gxx * Gyy * Gzz + Gxy * Gyz * Gxz + Gxz * Gxy * Gyz - Gxz * Gyy * Gxz - Gxy * Gxy * Gzz -
+                   Gxx * Gyz * Gyz;
+    const double gupxx = (Gyy * Gzz - Gyz * Gyz) / gupzz;
+    const double gupxy = -(Gxy * Gzz - Gyz * Gxz) / gupzz;
+    const double gupxz = (Gxy * Gyz - Gyy * Gxz) / gupzz;
+    const double gupyy = (Gxx * Gzz - Gxz * Gxz) / gupzz;
+    const double gupyz = -(Gxx * Gyz - Gxy * Gxz) / gupzz;
+    gupzz = (Gxx * Gyy - Gxy * Gxy) / gupzz;
+    const double aupxx = gupxx * axx + gupxy * axy + gupxz * axz;
+    const double aupxy = gupxx * axy + gupxy * ayy + gupxz * ayz;
+    const double aupxz = gupxx * axz + gupxy * ayz + gupxz * azz;
+    const double aupyx = gupxy * axx + gupyy * axy + gupyz * axz;
+    const double aupyy = gupxy * axy + gupyy * ayy + gupyz * ayz;
+    const double aupyz = gupxy * axz + gupyy * ayz + gupyz * azz;
+    const double aupzx = gupxz * axx + gupyz * axy + gupzz * axz;
+    const double aupzy = gupxz * axy + gupyz * ayy + gupzz * ayz;
+    const double aupzz = gupxz * axz + gupyz * ayz + gupzz * azz;
+    // 1/8pi \int psi^6 (x^a A^m_b - x^b A^m_a) dS_m
+    if (sym == 0) {
+      sx = sx + f1o8 * Psi * (nx * (Y * aupxz - Z * aupxy) + ny * (Y * aupyz - Z * aupyy) + nz * (Y * aupzz - Z * aupzy)) * w;
+      sy = sy + f1o8 * Psi * (nx * (Z * aupxx - X * aupxz) + ny * (Z * aupyx - X * aupyz) + nz * (Z * aupzx - X * aupzz)) * w;
+    }
+    if (sym == 0 || sym == 1)
+      sz = sz + f1o8 * Psi * (nx * (X * aupxy - Y * aupxx) + ny * (X * aupyy - Y * aupyx) + nz * (X * aupzy - Y * aupzx)) * w;
+    axx = Chi * (axx + Gxx * TRK / 3.0);
+    axy = Chi * (axy + Gxy * TRK / 3.0);
+    axz = Chi * (axz + Gxz * TRK / 3.0);
+    ayy = Chi * (ayy + Gyy * TRK / 3.0);
+    ayz = Chi * (ayz + Gyz * TRK / 3.0);
+    azz = Chi * (azz + Gzz * TRK / 3.0);
+    axx = axx - TRK;
+    ayy = ayy - TRK;
+    azz = azz - TRK;
+    // 1/8pi \int psi^6 (K_mi - delta_mi K) dS^m
+    if (sym == 0 || sym == 1) {
+      px = px + f1o8 * Psi * (nx * axx + ny * axy + nz * axz) * w;
+      py = py + f1o8 * Psi * (nx * axy + ny * ayy + nz * ayz) * w;
+    }
+    if (sym == 0) pz = pz + f1o8 * Psi * (nx * axz + ny * ayz + nz * azz) * w;
+  }
+  out[0] = mass * rex * rex * S.dphi * S.factor;
+  out[1] = px * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
+  out[2] = py * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
+  out[3] = pz * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
+  out[4] = sx * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
+  out[5] = sy * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
+  out[6] = sz * rex * rex * S.dphi * (1.0 / M_PI) * S.factor;
   return 0;
 }
 

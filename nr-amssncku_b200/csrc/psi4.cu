@@ -1,8 +1,10 @@
-// psi4.cu -- wave extraction of the engine: the Newman-Penrose scalar Psi4 of
-// a level's current state (bssn_class::Compute_Psi4, bssn_class.C:6210-6298,
-// with getnp4, getnp4.f90:12-452: Psi4type 0, tetradtype 2, ABV 0) and the
-// host side of its spin-weight -2 decomposition on a coordinate sphere
-// (surface_integral::surf_Wave, surface_integral.C:197-377, GaussInt).
+// psi4.cu -- the analysis quantities of the engine: the Newman-Penrose scalar
+// Psi4 of a level's current state (bssn_class::Compute_Psi4,
+// bssn_class.C:6210-6298, with getnp4, getnp4.f90:12-452: Psi4type 0,
+// tetradtype 2, ABV 0), the ADM-mass integrand (admmass_bssn), and the host
+// side of their surface integrals on a coordinate sphere
+// (surface_integral::surf_Wave / surf_MassPAng, surface_integral.C:197-377,
+// 2247-2512, GaussInt).
 //
 // Two passes over the level's points, FP64 from the FP64 state whatever the
 // engine's precision: the RHS point function in its diagnostic form writes
@@ -206,6 +208,60 @@ __global__ void __launch_bounds__(kPsi4Threads) k_psi4(const StepBlock<T>* __res
     B.K[fs + p] = -ip / TWO;
   }
 }
+
+// admmass_bssn (fadmquantites_bssn.f90:5-65): the integrand of the ADM mass,
+// mass^i = (Gam^i / 8 + gup^ij d_j chi / (4 chi^1.25)) / (2 pi) (chi the
+// conformal factor, stored less 1), at every point of the level into the
+// accumulator's fields 2, 3, 4.  Like the reference's temporaries it is not
+// synchronised: a block's ghost cells keep its own values.
+template <typename T, bool SYMM>
+__global__ void __launch_bounds__(kPsi4Threads) k_admmass(const StepBlock<T>* __restrict__ blocks,
+                                                          const int2* __restrict__ tiles, int ntiles, int tile_pts) {
+  const double ONE = 1.0, F1o8 = 1.0 / 8.0;
+  const double F1o2pi = ONE / (2.0 * M_PI);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+  for (int e = threadIdx.x; e < tile_pts; e += blockDim.x) {
+    const int2 tile = tiles[t];
+    const StepBlock<T>& B = blocks[tile.x];
+    const long long p = (long long)tile.y + e;
+    if (p >= B.npts) continue;
+    const double* u = B.tl[B.lvl[0]];
+    const long long fs = B.b.fs;
+    auto q = make_pt<double, SYMM>(u, B.b, p);
+    const PointGates G = point_gates(B.b, q.i, q.j, q.k);
+    const Coefs<double> C{B.C.d, B.C.d};
+    double chix, chiy, chiz;
+    grad<double, F_CHI>(q, C, G.ord, chix, chiy, chiz);
+    const double gxx = u[F_GXX * fs + p] + ONE, gyy = u[F_GYY * fs + p] + ONE, gzz = u[F_GZZ * fs + p] + ONE;
+    const double gxy = u[F_GXY * fs + p], gxz = u[F_GXZ * fs + p], gyz = u[F_GYZ * fs + p];
+    double gupzz = gxx * gyy * gzz + gxy * gyz * gxz + gxz * gxy * gyz - gxz * gyy * gxz - gxy * gxy * gzz -
+                   gxx * gyz * gyz;
+    const double gupxx = (gyy * gzz - gyz * gyz) / gupzz;
+    const double gupxy = -(gxy * gzz - gyz * gxz) / gupzz;
+    const double gupxz = (gxy * gyz - gyy * gxz) / gupzz;
+    const double gupyy = (gxx * gzz - gxz * gxz) / gupzz;
+    const double gupyz = -(gxx * gyz - gxy * gxz) / gupzz;
+    gupzz = (gxx * gyy - gxy * gxy) / gupzz;
+    const double f = 1.0 / 4.0 / pow(u[F_CHI * fs + p] + ONE, 1.25);
+    B.K[2 * fs + p] = (F1o8 * u[F_GAMX * fs + p] + f * (gupxx * chix + gupxy * chiy + gupxz * chiz)) * F1o2pi;
+    B.K[3 * fs + p] = (F1o8 * u[F_GAMY * fs + p] + f * (gupxy * chix + gupyy * chiy + gupyz * chiz)) * F1o2pi;
+    B.K[4 * fs + p] = (F1o8 * u[F_GAMZ * fs + p] + f * (gupxz * chix + gupyz * chiy + gupzz * chiz)) * F1o2pi;
+  }
+}
+
+template <typename T>
+cudaError_t launch_admmass(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm, cudaStream_t s) {
+  const StepBlock<T>* bl = (const StepBlock<T>*)table;
+  const int g = ntiles < 148 * 8 ? ntiles : 148 * 8;
+  if (symm)
+    k_admmass<T, true><<<g, kPsi4Threads, 0, s>>>(bl, tiles, ntiles, tile_pts);
+  else
+    k_admmass<T, false><<<g, kPsi4Threads, 0, s>>>(bl, tiles, ntiles, tile_pts);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_admmass<double>(const void*, const int2*, int, int, bool, cudaStream_t);
+template cudaError_t launch_admmass<float>(const void*, const int2*, int, int, bool, cudaStream_t);
 
 // Psi4 of every point of a level into its blocks' accumulators (fields 0, 1);
 // scratch holds 24 fields of the level's D layout.

@@ -205,3 +205,38 @@ void oracle_getnp4(const int *ex, const double *X, const double *Y, const double
     for (int a = 0; a < 8; ++a)
         for (int b = 0; b < 3; ++b) free(d[a][b]);
 }
+
+/* fadmquantites_bssn.f90:5-65 admmass_bssn: the ADM-mass integrand
+ * mass^i = (Gam^i / 8 + gup^ij chi_j / (4 (chi + 1)^1.25)) / (2 pi). */
+void oracle_admmass_bssn(const int *ex, const double *X, const double *Y, const double *Z,
+                         const double *chi, const double *dxx, const double *gxy, const double *gxz,
+                         const double *dyy, const double *gyz, const double *dzz,
+                         const double *Gamx, const double *Gamy, const double *Gamz,
+                         double *massx, double *massy, double *massz, int symmetry)
+{
+    const double ONE = 1.0, F1o8 = 1.0 / 8.0, SYM = 1.0;
+    const double PI = acos(-ONE);
+    const double F1o2pi = ONE / (2.0 * PI);
+    const long n = npts3(ex);
+    double *chix = oalloc(n), *chiy = oalloc(n), *chiz = oalloc(n);
+    oracle_fderivs(ex, chi, chix, chiy, chiz, X, Y, Z, SYM, SYM, SYM, symmetry);
+    for (long p = 0; p < n; ++p) {
+        const double gxx = dxx[p] + ONE, gyy = dyy[p] + ONE, gzz = dzz[p] + ONE;
+        const double Gxy = gxy[p], Gxz = gxz[p], Gyz = gyz[p];
+        double gupzz = gxx * gyy * gzz + Gxy * Gyz * Gxz + Gxz * Gxy * Gyz -
+                       Gxz * gyy * Gxz - Gxy * Gxy * gzz - gxx * Gyz * Gyz;
+        const double gupxx = (gyy * gzz - Gyz * Gyz) / gupzz;
+        const double gupxy = -(Gxy * gzz - Gyz * Gxz) / gupzz;
+        const double gupxz = (Gxy * Gyz - gyy * Gxz) / gupzz;
+        const double gupyy = (gxx * gzz - Gxz * Gxz) / gupzz;
+        const double gupyz = -(gxx * Gyz - Gxy * Gxz) / gupzz;
+        gupzz = (gxx * gyy - Gxy * Gxy) / gupzz;
+        const double f = 1 / 4.0 / pow(chi[p] + ONE, 1.25);
+        massx[p] = (F1o8 * Gamx[p] + f * (gupxx * chix[p] + gupxy * chiy[p] + gupxz * chiz[p])) * F1o2pi;
+        massy[p] = (F1o8 * Gamy[p] + f * (gupxy * chix[p] + gupyy * chiy[p] + gupyz * chiz[p])) * F1o2pi;
+        massz[p] = (F1o8 * Gamz[p] + f * (gupxz * chix[p] + gupyz * chiy[p] + gupzz * chiz[p])) * F1o2pi;
+    }
+    free(chix);
+    free(chiy);
+    free(chiz);
+}

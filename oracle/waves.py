@@ -209,3 +209,103 @@ def extract(H, level, psi4, rex, nquarter, maxl, symmetry=0):
     if not all(found):
         raise ValueError("a sphere point lies outside the level")
     return surf_wave(rex, vals, nquarter, symmetry, maxl)
+
+
+def admmass(X, Y, Z, state, symmetry=0):
+    """admmass_bssn (fadmquantites_bssn.f90:5-65) on one block: (3, ez, ey, ex)."""
+    L = O.lib()
+    shp = state.shape[1:]
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    out = np.zeros((3,) + shp)
+    X, Y, Z = (np.ascontiguousarray(v, dtype=np.float64) for v in (X, Y, Z))
+    f = [0, 2, 3, 4, 5, 6, 7, 14, 15, 16]   # chi, the metric, Gam^i
+    L.oracle_admmass_bssn(O._ex(shp), O._p(X), O._p(Y), O._p(Z), *[O._p(st[k]) for k in f],
+                          O._p(out[0]), O._p(out[1]), O._p(out[2]), ctypes.c_int(symmetry))
+    return out
+
+
+# the shift's parities for mass^i; the state's for chi .. A~zz (bssn_class.C:209-232)
+MASS_SOA = [(-1.0, 1.0, 1.0), (1.0, -1.0, 1.0), (1.0, 1.0, -1.0)]
+STATE_SOA = {0: (1, 1, 1), 1: (1, 1, 1), 2: (1, 1, 1), 3: (-1, -1, 1), 4: (-1, 1, -1), 5: (1, 1, 1), 6: (1, -1, -1),
+             7: (1, 1, 1), 8: (1, 1, 1), 9: (-1, -1, 1), 10: (-1, 1, -1), 11: (1, 1, 1), 12: (1, -1, -1),
+             13: (1, 1, 1)}
+
+
+def surf_masspang(rex, values, nquarter, symmetry):
+    """surface_integral.C:2247-2512 (GaussInt) given the 17 interpolated values
+    per sphere point (mass^x, mass^y, mass^z, chi, trK, gxx .. gzz, Axx .. Azz):
+    [mass, Px, Py, Pz, Sx, Sy, Sz]."""
+    ct, wt, n_theta, n_phi, dphi, pts = sphere(nquarter, symmetry)
+    factor = {0: 1, 1: 2, 2: 8}[symmetry]
+    f1o8 = 0.125
+    mass = ax = ay = az = px = py = pz = 0.0
+    for n in range(n_theta * n_phi):
+        i = n // n_phi
+        nx, ny, nz = pts[n]
+        X, Y, Z = rex * nx, rex * ny, rex * nz
+        s = values[n]
+        Chi, TRK = s[3], s[4]
+        Gxx, Gxy, Gxz, Gyy, Gyz, Gzz = s[5] + 1.0, s[6], s[7], s[8] + 1.0, s[9], s[10] + 1.0
+        axx, axy, axz, ayy, ayz, azz = s[11], s[12], s[13], s[14], s[15], s[16]
+        Chi = 1.0 / (1.0 + Chi)
+        Psi = Chi * math.sqrt(Chi)
+        mass = mass + (s[0] * nx + s[1] * ny + s[2] * nz) * wt[i]
+        gupzz = Gxx * Gyy * Gzz + Gxy * Gyz * Gxz + Gxz * Gxy * Gyz - Gxz * Gyy * Gxz - Gxy * Gxy * Gzz - Gxx * Gyz * Gyz
+        gupxx = (Gyy * Gzz - Gyz * Gyz) / gupzz
+        gupxy = -(Gxy * Gzz - Gyz * Gxz) / gupzz
+        gupxz = (Gxy * Gyz - Gyy * Gxz) / gupzz
+        gupyy = (Gxx * Gzz - Gxz * Gxz) / gupzz
+        gupyz = -(Gxx * Gyz - Gxy * Gxz) / gupzz
+        gupzz = (Gxx * Gyy - Gxy * Gxy) / gupzz
+        aupxx = gupxx * axx + gupxy * axy + gupxz * axz
+        aupxy = gupxx * axy + gupxy * ayy + gupxz * ayz
+        aupxz = gupxx * axz + gupxy * ayz + gupxz * azz
+        aupyx = gupxy * axx + gupyy * axy + gupyz * axz
+        aupyy = gupxy * axy + gupyy * ayy + gupyz * ayz
+        aupyz = gupxy * axz + gupyy * ayz + gupyz * azz
+        aupzx = gupxz * axx + gupyz * axy + gupzz * axz
+        aupzy = gupxz * axy + gupyz * ayy + gupzz * ayz
+        aupzz = gupxz * axz + gupyz * ayz + gupzz * azz
+        if symmetry == 0:
+            ax = ax + f1o8 * Psi * (nx * (Y * aupxz - Z * aupxy) + ny * (Y * aupyz - Z * aupyy) +
+                                    nz * (Y * aupzz - Z * aupzy)) * wt[i]
+            ay = ay + f1o8 * Psi * (nx * (Z * aupxx - X * aupxz) + ny * (Z * aupyx - X * aupyz) +
+                                    nz * (Z * aupzx - X * aupzz)) * wt[i]
+        if symmetry in (0, 1):
+            az = az + f1o8 * Psi * (nx * (X * aupxy - Y * aupxx) + ny * (X * aupyy - Y * aupyx) +
+                                    nz * (X * aupzy - Y * aupzx)) * wt[i]
+        axx = Chi * (axx + Gxx * TRK / 3.0)
+        axy = Chi * (axy + Gxy * TRK / 3.0)
+        axz = Chi * (axz + Gxz * TRK / 3.0)
+        ayy = Chi * (ayy + Gyy * TRK / 3.0)
+        ayz = Chi * (ayz + Gyz * TRK / 3.0)
+        azz = Chi * (azz + Gzz * TRK / 3.0)
+        axx = axx - TRK
+        ayy = ayy - TRK
+        azz = azz - TRK
+        if symmetry in (0, 1):
+            px = px + f1o8 * Psi * (nx * axx + ny * axy + nz * axz) * wt[i]
+            py = py + f1o8 * Psi * (nx * axy + ny * ayy + nz * ayz) * wt[i]
+        if symmetry == 0:
+            pz = pz + f1o8 * Psi * (nx * axz + ny * ayz + nz * azz) * wt[i]
+    sc = lambda v: v * rex * rex * dphi * (1.0 / PI) * factor   # noqa: E731
+    return [mass * rex * rex * dphi * factor, sc(px), sc(py), sc(pz), sc(ax), sc(ay), sc(az)]
+
+
+def adm_extract(H, level, states, rex, nquarter, symmetry=0):
+    """surf_MassPAng on a level: admmass_bssn per block (not synchronised),
+    the 17 values interpolated on the sphere, the sums."""
+    ids = [bi for p in H.levels[level] for bi in p.blocks]
+    comb = {}
+    for bi in ids:
+        b = H.blocks[bi]
+        X, Y, Z = H.coords(b)
+        comb[bi] = np.concatenate([admmass(X, Y, Z, states[bi], symmetry), states[bi][:14]])
+    _, _, _, _, _, pts = sphere(nquarter, symmetry)
+    P = OI.hierarchy_patches(H, level, comb)
+    soas = MASS_SOA + [STATE_SOA[k] for k in range(14)]
+    vals, found = OI.interp_points(P, [(rex * a, rex * b, rex * c) for a, b, c in pts], list(range(17)), soas,
+                                   symmetry)
+    if not all(found):
+        raise ValueError("a sphere point lies outside the level")
+    return surf_masspang(rex, vals, nquarter, symmetry)

@@ -124,5 +124,36 @@ def test_octant_modes_match_oracle():
         ms = max(np.abs(rp0).max(), np.abs(ip0).max())
         assert np.abs(rp - np.array(rp0)).max() <= 1e-10 * ms
         assert np.abs(ip - np.array(ip0)).max() <= 1e-10 * ms
+        # the ADM mass with the octant's factor 8 (the momenta are not integrated)
+        comb = np.concatenate([W.admmass(X, X, X, st, symmetry=2), st[:14]])
+        patches = [(bbox, [n, n, n], 0, [(bbox, X, X, X, comb)])]
+        vals, _ = OI.interp_points(patches, [(rex * a, rex * b_, rex * c) for a, b_, c in pts], list(range(17)),
+                                   W.MASS_SOA + [W.STATE_SOA[k] for k in range(14)], 2)
+        ref = np.array(W.surf_masspang(rex, vals, 4, 2))
+        got = e.adm_integrals(0, rex, nquarter=4)
+        assert abs(got[0] - ref[0]) <= 1e-10 * abs(ref[0]) and np.all(got[1:] == 0.0)
+    finally:
+        e.close()
+
+
+def test_adm_integrals_match_oracle(case):
+    """surf_MassPAng: the mass integrand formed per block (not synchronised),
+    17 values interpolated on the sphere, the sums; levels 0 and 1."""
+    H, init = case
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
+    try:
+        for i, st in enumerate(init):
+            e.set_state(i, st)
+        states = {i: init[i] for i in range(len(H.blocks))}
+        for lv, rex in ((0, 6.0), (1, 2.0)):
+            ref = np.array(W.adm_extract(H, lv, states, rex, nquarter=4))
+            got = e.adm_integrals(lv, rex, nquarter=4)
+            scale = np.abs(ref).max()
+            assert np.abs(got - ref).max() <= 1e-10 * scale, (lv, got, ref)
+        # the Psi4 fields survive the ADM integrand in the accumulator
+        e.psi4(0)
+        before = e.get_psi4(0)
+        e.adm_integrals(0, 6.0, nquarter=4)
+        assert np.array_equal(e.get_psi4(0), before)
     finally:
         e.close()

@@ -86,3 +86,36 @@ def test_surf_wave_recovers_known_modes(nquarter):
     for k, lm in enumerate(modes):
         assert abs(rp[k] - rex * coef[lm].real) < 1e-12 * rex
         assert abs(ip[k] - rex * coef[lm].imag) < 1e-12 * rex
+
+
+def _adm_single_block(masses, pos, mom=None, spin=None, rex=3.0, n=48, L=6.0, nquarter=8):
+    import interp as OI
+    X = O.cell_coords(-L, L, n)
+    st = O.get_lousto_nbhs(X, X, X, masses, pos, mom, spin)
+    comb = np.concatenate([W.admmass(X, X, X, st), st[:14]])
+    bb = [-L] * 3 + [L] * 3
+    patches = [(bb, [n] * 3, 0, [(bb, X, X, X, comb)])]
+    _, _, _, _, _, pts = W.sphere(nquarter, 0)
+    vals, found = OI.interp_points(patches, [(rex * a, rex * b, rex * c) for a, b, c in pts], list(range(17)),
+                                   W.MASS_SOA + [W.STATE_SOA[k] for k in range(14)], 0)
+    assert all(found)
+    return W.surf_masspang(rex, vals, nquarter, 0)
+
+
+def test_adm_mass_of_a_puncture():
+    """Brill-Lindquist: the mass integrand is -d_i psi / (2 pi), and psi is
+    harmonic, so the sphere gives the bare mass at any radius."""
+    out = _adm_single_block([1.0], [[0.0, 0.0, 0.0]])
+    assert abs(out[0] - 1.0) < 1e-4
+    assert max(abs(v) for v in out[1:]) < 1e-12
+
+
+def test_adm_momentum_and_spin_of_a_boosted_spinning_puncture():
+    """Bowen-York momentum and spin: the reference's integrand carries psi^6
+    K_ij = psi^4 A^_ij, so at radius r the momentum reads P (1 + M/2r)^4, and
+    the spin S (to the accuracy of the approximate data)."""
+    P, S, r = 0.1, 0.2, 3.0
+    out = _adm_single_block([1.0], [[0.0, 0.0, 0.0]], [[P, 0.0, 0.0]], [[0.0, 0.0, S]], rex=r)
+    assert abs(out[1] / (P * (1 + 1.0 / (2 * r)) ** 4) - 1) < 0.05
+    assert abs(out[6] / S - 1) < 0.05
+    assert max(abs(out[2]), abs(out[3]), abs(out[4]), abs(out[5])) < 1e-3 * P
