@@ -324,6 +324,12 @@ long long amss_engine_launch_count(amss_engine* e);
  * cell of its patch box; an AMR block its owned cells inside its patch,
  * buffer cells included.  Waits for the engine's stream. */
 int amss_engine_constraint_norms(amss_engine* e, int level, double norms[8]);
+/* The same norms over the level's first patch only, as the reference's
+ * Constraint_Out takes them (Parallel::L2Norm(GH->PatL[lev]->data, ...),
+ * bssn_class.C:7475): the first block's patch, or for blocks added by bbox
+ * those sharing its patch box.  Equal to amss_engine_constraint_norms on a
+ * level of one patch. */
+int amss_engine_constraint_norms_first_patch(amss_engine* e, int level, double norms[8]);
 
 /* Values of fields at points of one level (Parallel::PatList_Interp_Points,
  * Parallel.C:5614-5667, with Patch::Interp_Points, MPatch.C:339-500, and

@@ -191,13 +191,15 @@ class Engine:
     def run_graph(self, level, dt, nsteps, replays=1):
         check(lib().amss_engine_run_graph(self._h, level, dt, nsteps, replays), "amss_engine_run_graph")
 
-    def constraint_norms(self, level):
+    def constraint_norms(self, level, first_patch=False):
         """L2 norms of the Hamiltonian, momentum (x, y, z) and Gamma (x, y, z)
         constraints and of Theta (Z4c; 0 for BSSN) of a level's current state
-        (Parallel::L2Norm, Parallel.C:4214-4243), as a float64 array of 8."""
+        (Parallel::L2Norm, Parallel.C:4214-4243), as a float64 array of 8.
+        Over every patch of the level, or with first_patch over its first
+        patch only, as the reference's Constraint_Out takes them."""
         out = np.zeros(8)
-        check(lib().amss_engine_constraint_norms(self._h, level, out.ctypes.data_as(_DP)),
-              "amss_engine_constraint_norms")
+        fn = lib().amss_engine_constraint_norms_first_patch if first_patch else lib().amss_engine_constraint_norms
+        check(fn(self._h, level, out.ctypes.data_as(_DP)), "amss_engine_constraint_norms")
         return out
 
     def constraint_sums(self, level):

@@ -16,7 +16,11 @@ File format and cadence follow the reference:
   adds the coarse step dT * 0.5^max(0, trfls) to LastConsOut; once that reaches
   AnasTime, one line per level (levels in order, all at the same PhysTime) with
   the 7 norms of Parallel::L2Norm, and LastConsOut goes back to 0.  A Z4c run
-  writes 8 values per line, Theta's norm last (Z4c_class.C:2502-2511).
+  writes 8 values per line, Theta's norm last (Z4c_class.C:2502-2511).  The
+  reference takes the norms over the first patch of each level
+  (Parallel::L2Norm(GH->PatL[lev]->data, ...), bssn_class.C:7475), and so does
+  ConstraintMonitor by default; first_patch=False sums every patch, which
+  differs on levels of two or more patches.
 * bssn_psi4.dat (bssn_class.C:76-88 header, :7143-7263 AnalysisStuff): the
   column header names R{l:02d}m{m:03d} and I{l:02d}m{m:03d} for l = 2..maxl,
   m = -l..l, each in a field of 16 after "# time" in a field of 15; one line
@@ -50,7 +54,8 @@ class ConstraintMonitor:
     interval (AnasTime), `trfls` the level below which there is no time
     refinement (0 on the engine's hierarchies), `z4c` adds Theta's column."""
 
-    def __init__(self, out_dir, anas_time, name="bssn_constraint.dat", trfls=0, z4c=False):
+    def __init__(self, out_dir, anas_time, name="bssn_constraint.dat", trfls=0, z4c=False, first_patch=True):
+        self.first_patch = first_patch
         self.path = open_name(out_dir, name)
         self.anas_time = float(anas_time)
         self.trfls = int(trfls)
@@ -65,7 +70,7 @@ class ConstraintMonitor:
         """One line per level of the engine's current state at phys_time."""
         with open(self.path, "a") as f:
             for lv in range(nlevels):
-                c = engine.constraint_norms(lv)
+                c = engine.constraint_norms(lv, first_patch=self.first_patch)
                 f.write(format_line(phys_time, c[:self.nvals]) + "\n")
 
     def after_step(self, engine, phys_time, dT, nlevels):

@@ -130,6 +130,7 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.ditems) cudaFree(L.ditems);
     if (L.dfaces) cudaFree(L.dfaces);
     if (L.dregion) cudaFree(L.dregion);
+    if (L.dregion_first) cudaFree(L.dregion_first);
   }
   release_xfers(e);
   if (e->dblocks) cudaFree(e->dblocks);
@@ -367,9 +368,23 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
       }
     }
     if (L.dregion) cudaFree(L.dregion);
+    if (L.dregion_first) cudaFree(L.dregion_first);
+    L.dregion = L.dregion_first = nullptr;
     if (!reg.empty()) {
       AMSS_CK(cudaMalloc(&L.dregion, reg.size() * sizeof(int)));
       AMSS_CK(cudaMemcpy(L.dregion, reg.data(), reg.size() * sizeof(int), cudaMemcpyHostToDevice));
+      // the level's first patch (Parallel::L2Norm of GH->PatL[lev]->data, bssn_class.C:7475): the
+      // first block's engine patch, or for blocks added by bbox those sharing its patch box
+      const EBlock& f0 = e->blocks[L.blocks[0]];
+      for (size_t m = 0; m < L.own.size(); ++m) {
+        const EBlock& b = e->blocks[L.own[m]];
+        const bool first = f0.l2_by_bbox ? (b.l2_by_bbox && std::memcmp(b.pbbox, f0.pbbox, sizeof b.pbbox) == 0)
+                                         : b.patch == f0.patch;
+        if (!first)
+          for (int c = 0; c < 6; ++c) reg[6 * m + c] = 0;
+      }
+      AMSS_CK(cudaMalloc(&L.dregion_first, reg.size() * sizeof(int)));
+      AMSS_CK(cudaMemcpy(L.dregion_first, reg.data(), reg.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
   }
   L.dfs = doff;
@@ -1016,7 +1031,21 @@ extern "C" long long amss_engine_level_points(amss_engine* e, int level) {
   return n;
 }
 
+static int constraint_sums(amss_engine* e, int level, double* sums, bool first_patch);
+
 extern "C" int amss_engine_constraint_sums(amss_engine* e, int level, double* sums) {
+  return constraint_sums(e, level, sums, false);
+}
+
+extern "C" int amss_engine_constraint_norms_first_patch(amss_engine* e, int level, double* norms) {
+  if (!norms) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_norms_first_patch: null argument");
+  double s[8];
+  if (int rc = constraint_sums(e, level, s, true)) return rc;
+  for (int c = 0; c < 8; ++c) norms[c] = std::sqrt(s[c]);
+  return 0;
+}
+
+static int constraint_sums(amss_engine* e, int level, double* sums, bool first_patch) {
   if (!e || !sums) return amss_fail(AMSS_ERR_ARG, "amss_engine_constraint_sums: null argument");
   if (!e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_constraint_sums: commit the engine first");
   auto it = e->levels.find(level);
@@ -1038,10 +1067,12 @@ extern "C" int amss_engine_constraint_sums(amss_engine* e, int level, double* su
   const int tile_pts = e->prm.kernel == 0 ? (int)kPointwiseTile : 128;
   const cudaError_t err =
       e->prm.precision == 1
-          ? launch_constraints<float>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, L.dregion, e->cons, L.dfs,
-                                      e->cpart, kGrid, e->stream)
-          : launch_constraints<double>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm, L.dregion, e->cons, L.dfs,
-                                       e->cpart, kGrid, e->stream);
+          ? launch_constraints<float>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm,
+                                      first_patch ? L.dregion_first : L.dregion, e->cons, L.dfs, e->cpart, kGrid,
+                                      e->stream)
+          : launch_constraints<double>(L.dtable, L.dtiles, L.ntiles, tile_pts, L.symm,
+                                       first_patch ? L.dregion_first : L.dregion, e->cons, L.dfs, e->cpart, kGrid,
+                                       e->stream);
   AMSS_CK(err);
   e->launches += 2;
   std::vector<double> part((size_t)kGrid * 8);
@@ -1476,6 +1507,13 @@ extern "C" int amss_engine_set_punctures(amss_engine* e, int n, const double* po
   e->ntrack = 0;
   if (n == 0) return 0;
   const int level = e->levels.rbegin()->first;
+  // the reference drops the buffer on a patch side moved onto a symmetry plane
+  // (MPatch.C:79-116); the engine's patches carry one buffer width on every side
+  if (e->prm.symmetry > 0)
+    for (int pid : e->levels[level].patches)
+      if (e->patches[pid].buffer > 0)
+        return amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_set_punctures: symmetry planes with buffered refined "
+                                               "patches on the finest level are not supported");
   const std::vector<IPatch> ps = level_patches(e, e->levels[level]);
   std::vector<TrackPatch> tp;
   std::vector<TrackBlock> tb;

@@ -124,6 +124,7 @@ struct ELevel {
   int zsplit = 1;               // z-slabs per block in the stencil pass
   long long dfs = 0;            // slot stride of D for this level
   int* dregion = nullptr;       // per table block: local [lo, hi) of its owned cells inside its patch
+  int* dregion_first = nullptr; // the same, empty for blocks outside the level's first patch
   int cur = 0;                  // host mirror of the ring index
   long long steps = 0;
 };

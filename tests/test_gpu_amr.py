@@ -95,12 +95,12 @@ def test_mixed_amr_error_bound(fp64_reference):
 import oracle as O
 
 
-def _oracle_level_norms(H, states, level):
+def _oracle_level_norms(H, states, level, patch=None):
     """sqrt(sum c^2 dV) over the owned cells of the level's blocks inside their
     patch (buffer included), residuals from the oracle's compute_rhs_bssn co=0."""
     sums = np.zeros(7)
     for i, b in enumerate(H.blocks):
-        if b.level != level:
+        if b.level != level or (patch is not None and b.patch != patch):
             continue
         X, Y, Z = H.coords(b)
         cons = O.compute_rhs_bssn(X, Y, Z, states[i], co=0, eps=0.1)[4]
@@ -130,6 +130,30 @@ def test_constraint_norms_match_oracle(precision):
         np.testing.assert_allclose(got[:7], ref, rtol=1e-12, atol=0)
         assert got[7] == 0.0
     e.close()
+
+
+def test_constraint_norms_first_patch():
+    """Constraint_Out takes each level's first patch only (bssn_class.C:7475):
+    on a level of two patches the first-patch norms are those of patch 0's
+    blocks, the all-patch norms add patch 1's."""
+    H = box_in_box(40, 10.0, [(4.5, 0.5, 0.0), (-4.5, -0.5, 0.0)], 2, box_cells=16, seed=2, block_min=10,
+                   block_max=16)
+    assert len(H.levels[1]) == 2
+    init = OA.initial_state(H, [0.5, 0.5], [[4.5, 0.5, 0.0], [-4.5, -0.5, 0.0]], noise=1e-6)
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
+    try:
+        for i, st in enumerate(init):
+            e.set_state(i, st)
+        states = [e.get_state(i) for i in range(len(H.blocks))]
+        got = e.constraint_norms(1, first_patch=True)
+        np.testing.assert_allclose(got[:7], _oracle_level_norms(H, states, 1, patch=0), rtol=1e-12, atol=0)
+        allp = e.constraint_norms(1)
+        np.testing.assert_allclose(allp[:7], _oracle_level_norms(H, states, 1), rtol=1e-12, atol=0)
+        assert np.all(allp[:7] > got[:7])
+        # one patch: the two agree
+        np.testing.assert_array_equal(e.constraint_norms(0, first_patch=True), e.constraint_norms(0))
+    finally:
+        e.close()
 
 
 def test_z4c_constraint_norms_match_oracle():

@@ -52,7 +52,8 @@ class _FakeEngine:
     def __init__(self):
         self.calls = []
 
-    def constraint_norms(self, level):
+    def constraint_norms(self, level, first_patch=False):
+        assert first_patch   # the monitor file takes the reference's first patch by default
         self.calls.append(level)
         return np.arange(8, dtype=float) + 10.0 * level + 0.5
 
