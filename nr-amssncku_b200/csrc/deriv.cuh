@@ -32,6 +32,15 @@ namespace amss {
 // (deriv_tile) so that narrow blocks do not leave lanes idle: W = the block's
 // x extent split into pieces of at most 64, H = DTHREADS / W rows.
 constexpr int DTHREADS = 256;
+// Resident CTAs of DTHREADS threads the stencil pass is compiled for, FP64 and
+// FP32 arithmetic: 64 and 80 registers (the window spills a few hundred bytes
+// to L1), against 128 at two CTAs -- more warps to cover the plane loads.
+#ifndef AMSS_DERIV_MINB_F64
+#define AMSS_DERIV_MINB_F64 4
+#endif
+#ifndef AMSS_DERIV_MINB_F32
+#define AMSS_DERIV_MINB_F32 3
+#endif
 #ifndef AMSS_DERIV_PREFETCH   // planes beyond the register fetch whose tile rows are prefetched into L2 (0: none)
 #define AMSS_DERIV_PREFETCH 4
 #endif
@@ -350,7 +359,7 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
 // Stencil pass over a work list of (block, tile, field) items, ordered by
 // field so that resident CTAs share one code path.
 template <typename T, typename SI>
-__global__ void __launch_bounds__(DTHREADS, 2) k_deriv(const StepBlock<T>* __restrict__ blocks,
+__global__ void __launch_bounds__(DTHREADS, sizeof(T) == 8 ? AMSS_DERIV_MINB_F64 : AMSS_DERIV_MINB_F32) k_deriv(const StepBlock<T>* __restrict__ blocks,
                                                       const DerivItem* __restrict__ items, int nitems, int sub,
                                                       T* __restrict__ D, long long dfs) {
   extern __shared__ __align__(16) unsigned char smem[];
