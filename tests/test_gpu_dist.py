@@ -74,6 +74,15 @@ def test_ranks_equal_one_engine(case, precision, nranks, mode):
         assert np.allclose(a, b, rtol=1e-12, atol=0)
 
 
+def test_z4c_ranks_equal_one_engine(case):
+    """25 fields (Theta last): the staging regions follow the field count."""
+    H, init, dt0 = case
+    init25 = [np.concatenate([s, 1e-8 * np.ones((1,) + s.shape[1:])]) for s in init]
+    ref, _ = _single(H, init25, dt0, 1, formulation="z4c")
+    got, _, cross = _group(H, init25, dt0, 1, D.partition(H, 2), 2, formulation="z4c")
+    assert cross > 0 and all(np.array_equal(g, r) for g, r in zip(got, ref))
+
+
 def test_rank_without_blocks_on_a_level(case):
     """Rank 1 holds no block of the finest level: it still takes part in
     that level's exchanges (restriction into its level-1 blocks)."""
