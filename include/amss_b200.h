@@ -372,7 +372,9 @@ int amss_engine_get_punctures(amss_engine* e, double* pos);
  * compute_rhs_bssn outputs of the level).  The result lives in each block's
  * RK4 accumulator, fields 0 (Rpsi4) and 1 (Ipsi4), until the next step;
  * amss_engine_get_psi4 copies a block's two fields to the host (2 x npts).
- * BSSN engines only.
+ * A Z4c engine takes them from its first 24 fields, as Z4c_class inherits
+ * Compute_Psi4 (its Christoffel and Ricci outputs are ricci_gamma's, the
+ * BSSN formulas).
  *
  * amss_engine_psi4_modes: surface_integral::surf_Wave (surface_integral.C:
  * 197-377 with GaussInt; its sphere, :39-181): Psi4 interpolated on the
@@ -391,7 +393,7 @@ int amss_engine_psi4_modes(amss_engine* e, int level, double rex, int nquarter, 
  * quadrature, from the level's current state.  out[7]: mass, Px, Py, Pz, Sx,
  * Sy, Sz, the bssn_ADMQs.dat columns (Symmetry 1 gives only Px, Py, Sz of the
  * momenta, Symmetry 2 none; the others are 0).  Overwrites accumulator
- * fields 2-4 (Psi4 in fields 0, 1 stays).  BSSN engines only. */
+ * fields 2-4 (Psi4 in fields 0, 1 stays). */
 int amss_engine_adm_integrals(amss_engine* e, int level, double rex, int nquarter, double out[7]);
 
 /* ---- Blocks divided among ranks, one engine per GPU (Parallel::distribute,

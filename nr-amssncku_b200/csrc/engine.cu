@@ -1253,7 +1253,6 @@ extern "C" int amss_engine_interp_points(amss_engine* e, int level, int npts, co
 // current state on every point of its blocks, then the level's ghost sync.
 extern "C" int amss_engine_psi4(amss_engine* e, int level) {
   if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "amss_engine_psi4: commit the engine first");
-  if (e->nf != NFIELDS_BSSN) return amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_psi4: BSSN engines only (getnp4)");
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_psi4: no such level");
   ELevel& L = it->second;
@@ -1406,7 +1405,6 @@ extern "C" int amss_engine_adm_integrals(amss_engine* e, int level, double rex, 
   if (!out || !(rex > 0) || nquarter < 1)
     return amss_fail(AMSS_ERR_ARG, "amss_engine_adm_integrals: rex > 0, N >= 1 and an output array");
   if (int rc = check_whole(e, "amss_engine_adm_integrals")) return rc;
-  if (e->nf != NFIELDS_BSSN) return amss_fail(AMSS_ERR_UNSUPPORTED, "amss_engine_adm_integrals: BSSN engines only");
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_adm_integrals: no such level");
   ELevel& L = it->second;

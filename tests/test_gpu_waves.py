@@ -157,3 +157,23 @@ def test_adm_integrals_match_oracle(case):
         assert np.array_equal(e.get_psi4(0), before)
     finally:
         e.close()
+
+
+def test_z4c_engine_psi4_and_adm(case):
+    """A Z4c run's analysis reads the first 24 fields (Z4c_class inherits
+    Compute_Psi4 and AnalysisStuff); Theta does not enter."""
+    H, init = case
+    init25 = [np.concatenate([s, 1e-6 * np.ones((1,) + s.shape[1:])]) for s in init]
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1, formulation="z4c")
+    try:
+        for i, st in enumerate(init25):
+            e.set_state(i, st)
+        states = {i: init[i] for i in range(len(H.blocks))}
+        ref = W.psi4_level(H, 0, states, eps=0.1)
+        e.psi4(0)
+        scale = max(np.abs(r).max() for r in ref.values())
+        assert max(np.abs(e.get_psi4(bi) - ref[bi]).max() for bi in ref) <= 1e-10 * scale
+        adm = np.array(W.adm_extract(H, 0, states, 6.0, nquarter=4))
+        assert np.abs(e.adm_integrals(0, 6.0, nquarter=4) - adm).max() <= 1e-10 * np.abs(adm).max()
+    finally:
+        e.close()
