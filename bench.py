@@ -219,8 +219,9 @@ def time_engine(args, w, init, precision, rank, world, dev):
                                           formulation=args.formulation)
     for i, st in enumerate(init):
         eng.set_state(i, st)
-    for lv, (tw, zs, _) in tiling.items():
+    for lv, (tw, zs, oc, _) in tiling.items():
         eng.set_level_tiling(lv, tw, zs)
+        eng.set_level_occupancy(lv, oc)
     eng.set_punctures(w["pos"])   # Step tracks the punctures on the finest level (MAPBH 0)
     stream = torch.cuda.ExternalStream(eng.stream)
 
@@ -275,7 +276,7 @@ def time_engine(args, w, init, precision, rank, world, dev):
     eng.close()
     return dict(ms_per_step=ms / args.steps, e2e_ms=e2e_ms, launches=launches, clocks=clk.summary(),
                 nan=bool(nan), tracked=tracked,
-                tiling={str(lv): [tw, zs, round(t, 4)] for lv, (tw, zs, t) in tiling.items()})
+                tiling={str(lv): [tw, zs, oc, round(t, 4)] for lv, (tw, zs, oc, t) in tiling.items()})
 
 
 def roofline(precision, nf, zones, ms_per_step, npts, peak):
@@ -340,9 +341,10 @@ def run_ours(args, rank, world):
         "gpu_launches": int(r["launches"]),
         "clocks": r["clocks"],
         "nan": r["nan"],
-        "tiling": {"per_level": r["tiling"], "what": "stencil-pass tile width (0 = default) and z-slabs per block, "
-                                                    "and the tuner's ms per level step, chosen by amss_b200.autotune "
-                                                    "before the timed region"},
+        "tiling": {"per_level": r["tiling"], "what": "stencil-pass tile width (0 = default), z-slabs per block, "
+                                                    "occupancy form (0: 2 CTAs/SM, 1: 4 FP64 / 3 FP32) and the "
+                                                    "tuner's ms per level step, chosen by amss_b200.autotune before "
+                                                    "the timed region"},
         "punctures_after_warmup_and_timed_steps": r["tracked"],
     }
     if args.precision == "fp64" and args.formulation == "bssn" and not args.no_parts:

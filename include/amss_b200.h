@@ -288,6 +288,11 @@ int amss_engine_run_graph(amss_engine* e, int level, double dt, int nsteps, int 
 int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_w, int zsplit);
 /* The level's tiling (as set; 0 = default width) and its stencil work items. */
 int amss_engine_get_level_tiling(amss_engine* e, int level, int* tile_w, int* zsplit, int* nitems);
+/* No reference counterpart: which compiled form of the stencil pass a level
+ * uses, 0 (two resident CTAs per SM, the default) or 1 (four in FP64, three in
+ * FP32, fewer registers with some spills).  Results do not depend on it. */
+int amss_engine_set_level_occupancy(amss_engine* e, int level, int occ);
+int amss_engine_get_level_occupancy(amss_engine* e, int level, int* occ);
 
 /* Moving-box regrid (cgh::Regrid_Onelevel, cgh.C:1304-1506, whose data step is
  * cgh::recompose_cgh_Onelevel and Parallel::fill_level_data, Parallel.C).

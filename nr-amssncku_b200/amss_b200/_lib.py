@@ -110,6 +110,8 @@ def lib():
     L.amss_engine_psi4_modes.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          _DP, _DP]
     L.amss_engine_constraint_norms_first_patch.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+    L.amss_engine_set_level_occupancy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.amss_engine_get_level_occupancy.argtypes = [ctypes.c_void_p, ctypes.c_int, _IP]
     L.amss_engine_adm_integrals.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _DP]
     _lib = L
     return L

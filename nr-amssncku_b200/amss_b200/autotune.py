@@ -1,10 +1,12 @@
 """Autotuner of the stencil pass's tiling, per level.
 
 The stencil pass (k_deriv) runs one CTA per (field, x-y tile, z-slab) work
-item, two resident per SM.  How its items fill the GPU depends on each level's
-block shapes: the tile width W (H = 256 / W rows) sets the halo overhead and
-the item count, the z-split trades a 7-plane prologue per slab for more,
-shorter items that fill the last wave of CTAs better.  The tuner times each
+item.  How its items fill the GPU depends on each level's block shapes: the
+tile width W (H = 256 / W rows) sets the halo overhead and the item count, the
+z-split trades a 7-plane prologue per slab for more, shorter items that fill
+the last wave of CTAs better, and the occupancy form (two resident CTAs per SM,
+or four in FP64 / three in FP32 with fewer registers and some spills) trades
+spills for warps.  The tuner times each
 candidate on a scratch engine holding the same hierarchy and state (CUDA
 events around graph replays of that level's RK4 step; the live engine is not
 touched), keeps the fastest per level, and caches the choice in a JSON file
@@ -28,9 +30,9 @@ def level_key(H, level, precision, formulation):
 
 
 def candidates(H, level):
-    """(tile width, z-split) pairs worth timing for a level: the default
+    """(tile width, z-split, occupancy) worth timing for a level: the default
     width and the widths that cut the level's smallest block width into 1-3
-    near-equal tiles, each with 1-4 z-slabs."""
+    near-equal tiles, each with 1-4 z-slabs, in both occupancy forms."""
     wmin = min(H.blocks[i].ex[0] for p in H.levels[level] for i in p.blocks)
     widths = {0}
     for parts in (1, 2, 3):
@@ -40,7 +42,7 @@ def candidates(H, level):
     for w in (16, 32):
         if w <= wmin:
             widths.add(w)
-    return [(w, z) for w in sorted(widths) for z in (1, 2, 3, 4)]
+    return [(w, z, o) for w in sorted(widths) for z in (1, 2, 3, 4) for o in (0, 1)]
 
 
 def _time_level(eng, level, dt, reps):
@@ -58,8 +60,9 @@ def _time_level(eng, level, dt, reps):
 
 def tune(H, states, dt0, precision="fp64", formulation="bssn", eps=0.1, symmetry=0, cache=DEFAULT_CACHE,
          reps=3, levels=None):
-    """{level: (tile_w, zsplit, ms per step)} for the hierarchy, from the cache
-    where an entry exists, else measured on a scratch engine (and stored)."""
+    """{level: (tile_w, zsplit, occupancy, ms per step)} for the hierarchy,
+    from the cache where an entry exists, else measured on a scratch engine
+    (and stored)."""
     book = {}
     if cache and os.path.exists(cache):
         with open(cache) as f:
@@ -67,7 +70,7 @@ def tune(H, states, dt0, precision="fp64", formulation="bssn", eps=0.1, symmetry
     out, todo = {}, []
     for lv in (range(len(H.levels)) if levels is None else levels):
         k = level_key(H, lv, precision, formulation)
-        if k in book:
+        if k in book and len(book[k]) == 4:
             out[lv] = tuple(book[k])
         else:
             todo.append(lv)
@@ -77,14 +80,16 @@ def tune(H, states, dt0, precision="fp64", formulation="bssn", eps=0.1, symmetry
             for lv in todo:
                 dt = dt0 / 2 ** lv
                 best = None
-                for w, z in candidates(H, lv):
+                for w, z, o in candidates(H, lv):
                     for i, st in enumerate(states):
                         eng.set_state(i, st)
                     eng.set_level_tiling(lv, w, z)
+                    eng.set_level_occupancy(lv, o)
                     ms = _time_level(eng, lv, dt, reps)
-                    if best is None or ms < best[2]:
-                        best = (w, z, ms)
+                    if best is None or ms < best[3]:
+                        best = (w, z, o, ms)
                 eng.set_level_tiling(lv, 0, 1)
+                eng.set_level_occupancy(lv, 0)
                 out[lv] = best
                 book[level_key(H, lv, precision, formulation)] = list(best)
         finally:
@@ -97,6 +102,7 @@ def tune(H, states, dt0, precision="fp64", formulation="bssn", eps=0.1, symmetry
 
 
 def apply(eng, choices):
-    """Set the tuned tiling on a live engine."""
-    for lv, (w, z, _) in choices.items():
+    """Set the tuned tiling and occupancy on a live engine."""
+    for lv, (w, z, o, _) in choices.items():
         eng.set_level_tiling(lv, w, z)
+        eng.set_level_occupancy(lv, o)

@@ -181,6 +181,16 @@ class Engine:
         check(lib().amss_engine_set_level_tiling(self._h, level, int(tile_w), int(zsplit)),
               "amss_engine_set_level_tiling")
 
+    def set_level_occupancy(self, level, occ):
+        """Compiled form of a level's stencil pass: 0 (two resident CTAs per
+        SM) or 1 (four in FP64, three in FP32)."""
+        check(lib().amss_engine_set_level_occupancy(self._h, level, int(occ)), "amss_engine_set_level_occupancy")
+
+    def level_occupancy(self, level):
+        o = ctypes.c_int()
+        check(lib().amss_engine_get_level_occupancy(self._h, level, ctypes.byref(o)), "amss_engine_get_level_occupancy")
+        return o.value
+
     def level_tiling(self, level):
         """(tile width as set, z-slabs, stencil work items) of one level."""
         w, z, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -121,6 +121,7 @@ def regrid(eng, H, regridder, porg0=None):
             new.regrid_fill(eng, lv, back)
         w, z, _ = eng.level_tiling(lv)
         new.set_level_tiling(lv, w, z)
+        new.set_level_occupancy(lv, eng.level_occupancy(lv))
     if getattr(eng, "_ntrack", 0):
         new.set_punctures(porg0)
     eng.close()

@@ -41,7 +41,7 @@ cudaError_t launch_face(const void* blocks, const int2* faces, int nfaces, int s
                         unsigned* status, cudaStream_t s);
 template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
-                         int grid, cudaStream_t s);
+                         int grid, cudaStream_t s, int occ);
 
 // out = E(in) on the metric / A~ fields; other fields copied.
 __global__ void k_enforce_copy(const double* __restrict__ in, double* __restrict__ out, long long n, long long fs) {
@@ -153,7 +153,7 @@ int fwd_step(amss_adjoint* a, const double* U0raw, double* Unew, double* Z0, dou
   for (int sub = 0; sub < 4; ++sub) {
     const StepBlock<double>* T = a->dtab + sub;
     double* D = Dsub ? Dsub[sub] : a->D;
-    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, D, a->fs, std::min(a->nitems, 148 * 16), s)));
+    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, D, a->fs, std::min(a->nitems, 148 * 16), s, 0)));
     AMSS_CK((launch_substep<double, double, false, true, false>(T, a->dtiles, a->ntiles, sub, rk, 0, a->dstatus,
                                                               std::min(a->ntiles, 148 * 8), s, D, a->fs)));
     AMSS_CK((launch_face<double, double, false>(T, a->dfaces, a->nfaces, sub, rk, 0, a->dstatus, s)));
@@ -173,7 +173,7 @@ int rhs_vjp(amss_adjoint* a, int sub, const double* Xin, const double* Rbv, doub
   cudaStream_t s = a->stream;
   const StepBlock<double>* T = a->dtab + sub;
   if (!Dpre) {
-    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+    AMSS_CK((launch_deriv<double, double>(T, a->ditems, a->nitems, sub, a->D, a->fs, std::min(a->nitems, 148 * 16), s, 0)));
     a->launches++;
   }
   a->host_adj.D = Dpre ? Dpre : a->D;
@@ -344,7 +344,7 @@ static int loss_and_grad(amss_adjoint* a, double* loss, bool want_grad) {
   const int gw = 3;
   a->host_tab[0].tl[0] = a->U;   // stencil pass of U (substep-0 input)
   AMSS_CK(cudaMemcpyAsync(a->dtab, a->host_tab, sizeof(StepBlock<double>), cudaMemcpyHostToDevice, s));
-  AMSS_CK((launch_deriv<double, double>(a->dtab, a->ditems, a->nitems, 0, a->D, a->fs, std::min(a->nitems, 148 * 16), s)));
+  AMSS_CK((launch_deriv<double, double>(a->dtab, a->ditems, a->nitems, 0, a->D, a->fs, std::min(a->nitems, 148 * 16), s, 0)));
   a->host_adj.D = a->D;
   a->host_adj.X = a->U;
   a->host_adj.Rb = nullptr;

@@ -32,9 +32,12 @@ namespace amss {
 // (deriv_tile) so that narrow blocks do not leave lanes idle: W = the block's
 // x extent split into pieces of at most 64, H = DTHREADS / W rows.
 constexpr int DTHREADS = 256;
-// Resident CTAs of DTHREADS threads the stencil pass is compiled for, FP64 and
-// FP32 arithmetic: 64 and 80 registers (the window spills a few hundred bytes
-// to L1), against 128 at two CTAs -- more warps to cover the plane loads.
+// Resident CTAs of DTHREADS threads the stencil pass is compiled for.  Two
+// forms: occupancy 0, two CTAs (128 registers), and occupancy 1, four CTAs in
+// FP64 / three in FP32 arithmetic (64 / 80 registers; the windows spill a few
+// hundred bytes to L1): more warps to cover the plane loads, at the price of
+// the spills.  Which is faster depends on the level (the autotuner picks).
+constexpr int kDerivMinbLow = 2;
 #ifndef AMSS_DERIV_MINB_F64
 #define AMSS_DERIV_MINB_F64 4
 #endif
@@ -358,8 +361,8 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
 
 // Stencil pass over a work list of (block, tile, field) items, ordered by
 // field so that resident CTAs share one code path.
-template <typename T, typename SI>
-__global__ void __launch_bounds__(DTHREADS, sizeof(T) == 8 ? AMSS_DERIV_MINB_F64 : AMSS_DERIV_MINB_F32) k_deriv(const StepBlock<T>* __restrict__ blocks,
+template <typename T, typename SI, int MINB>
+__global__ void __launch_bounds__(DTHREADS, MINB) k_deriv(const StepBlock<T>* __restrict__ blocks,
                                                       const DerivItem* __restrict__ items, int nitems, int sub,
                                                       T* __restrict__ D, long long dfs) {
   extern __shared__ __align__(16) unsigned char smem[];

@@ -38,7 +38,7 @@ cudaError_t launch_face(const void* blocks, const int2* faces, int nfaces, int s
                         unsigned* status, cudaStream_t s);
 template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
-                         int grid, cudaStream_t s);
+                         int grid, cudaStream_t s, int occ);
 cudaError_t launch_enforce(long long n, long long fs, double* g, double* a, cudaStream_t s);
 template <typename T>
 cudaError_t launch_constraints(const void* table, const int2* tiles, int ntiles, int tile_pts, bool symm,
@@ -712,8 +712,9 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
       e->launches++;
     }
     if (split) {
-      const cudaError_t ed = mixed ? launch_deriv<float, float>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream)
-                                   : launch_deriv<double, double>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream);
+      const cudaError_t ed =
+          mixed ? launch_deriv<float, float>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc)
+                : launch_deriv<double, double>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc);
       AMSS_CK(ed);
       e->launches++;
     }
@@ -812,6 +813,23 @@ extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   return e->prm.precision == 1 ? patch_table_dw<float>(e, L) : patch_table_dw<double>(e, L);
+}
+
+extern "C" int amss_engine_set_level_occupancy(amss_engine* e, int level, int occ) {
+  if (!e || !e->committed || e->plan_only) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_occupancy: no such level");
+  if (occ != 0 && occ != 1) return amss_fail(AMSS_ERR_ARG, "amss_engine_set_level_occupancy: occupancy 0 or 1");
+  it->second.docc = occ;
+  return 0;
+}
+
+extern "C" int amss_engine_get_level_occupancy(amss_engine* e, int level, int* occ) {
+  if (!e || !e->committed || !occ) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_get_level_occupancy: no such level");
+  *occ = it->second.docc;
+  return 0;
 }
 
 extern "C" int amss_engine_get_level_tiling(amss_engine* e, int level, int* tile_w, int* zsplit, int* nitems) {

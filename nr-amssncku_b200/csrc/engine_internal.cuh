@@ -122,6 +122,7 @@ struct ELevel {
   int nditems = 0;
   int tile_w = 0;               // stencil-pass tile width (0: deriv_tile_w of each block's x extent)
   int zsplit = 1;               // z-slabs per block in the stencil pass
+  int docc = 0;                 // stencil-pass occupancy form: 0 two resident CTAs, 1 more (deriv.cuh)
   long long dfs = 0;            // slot stride of D for this level
   int* dregion = nullptr;       // per table block: local [lo, hi) of its owned cells inside its patch
   int* dregion_first = nullptr; // the same, empty for blocks outside the level's first patch

@@ -169,16 +169,21 @@ cudaError_t launch_substep(const void* blocks, const int2* tiles, int ntiles, in
   return cudaGetLastError();
 }
 
-// Stencil pass launcher: substep 0 reads the FP64 state, 1-3 the stages.
+// Stencil pass launcher: substep 0 reads the FP64 state, 1-3 the stages;
+// occ selects the compiled occupancy (0: two resident CTAs, 1: more).
 template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
-                         int grid, cudaStream_t s) {
+                         int grid, cudaStream_t s, int occ) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
   const size_t smem = kDerivSmem;   // < 48 KB: no opt-in attribute needed
-  if (sub == 0)
-    k_deriv<T, double><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
-  else
-    k_deriv<T, SS><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  constexpr int hi = sizeof(T) == 8 ? AMSS_DERIV_MINB_F64 : AMSS_DERIV_MINB_F32;
+  if (sub == 0) {
+    if (occ) k_deriv<T, double, hi><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+    else k_deriv<T, double, kDerivMinbLow><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  } else {
+    if (occ) k_deriv<T, SS, hi><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+    else k_deriv<T, SS, kDerivMinbLow><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
+  }
   return cudaGetLastError();
 }
 
