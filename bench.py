@@ -222,6 +222,9 @@ def time_engine(args, w, init, precision, rank, world, dev):
     for lv, (tw, zs, oc, _) in tiling.items():
         eng.set_level_tiling(lv, tw, zs)
         eng.set_level_occupancy(lv, oc)
+    if not tiling and args.occupancy is not None and args.kernel == "split":
+        for lv in range(len(H.levels)):
+            eng.set_level_occupancy(lv, args.occupancy)
     eng.set_punctures(w["pos"])   # Step tracks the punctures on the finest level (MAPBH 0)
     stream = torch.cuda.ExternalStream(eng.stream)
 
@@ -607,6 +610,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tune", type=int, default=1, help="pick each level's stencil-pass tiling with the autotuner")
     ap.add_argument("--tune-cache", default="", help="JSON cache of tuned tilings (default: none, tune every run)")
+    ap.add_argument("--occupancy", type=int, choices=[0, 1], default=None,
+                    help="with --tune 0: the stencil pass's occupancy form on every level (default: the engine's, 0)")
     ap.add_argument("--no-parts", action="store_true",
                     help="FP64 line only: skip the mixed-form and adjoint parts of the metric")
     ap.add_argument("--report", choices=["none", "mixed"], default="none",
