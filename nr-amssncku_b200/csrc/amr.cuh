@@ -64,8 +64,8 @@ __device__ __constant__ double kProlongW[6] = {7.7e1 / 8.192e3, -6.93e2 / 8.192e
 // One thread takes one field of a run of kProlongRun fine cells along x that
 // starts at an even index (cells outside the box are skipped).  The cells of a
 // run share their y and z weights, so the z-then-y reduction of each coarse x
-// column the run reads is formed once (10 columns for 8 cells instead of 6 per
-// cell) and the x sums of the cells reuse it: the same operations in the same
+// column the run reads is formed once (14 columns for 16 cells instead of 6
+// per cell) and the x sums of the cells reuse it: the same operations in the same
 // order as the cell-by-cell form.  Tiles count (field, run) units, field-major
 // within a box, not cells.
 __global__ void k_amr_prolong(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,

@@ -26,7 +26,7 @@ struct AmrBox {
 
 // Fine cells per thread of the prolongation (a run along x from an even
 // index), and the runs that cover x cells [lo0, lo0 + n0) of a box.
-constexpr int kProlongRun = 8;
+constexpr int kProlongRun = 16;
 __host__ __device__ inline int prolong_runs_x(int lo0, int n0) {
   return ((lo0 + n0) - (lo0 & ~1) + kProlongRun - 1) / kProlongRun;
 }
