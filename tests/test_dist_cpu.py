@@ -293,3 +293,20 @@ def test_plan_refuses_device_calls():
     with pytest.raises(AmssError):
         p.sync()
     p.close()
+
+
+def test_nccl_transport_resolves_without_a_gpu():
+    """The NCCL transport opens the libnccl already in the process (PyTorch's)
+    at run time; making the unique id rank 0 broadcasts needs no GPU.  Joining
+    a communicator needs a committed engine: a plan is refused."""
+    L = lib()
+    buf = ctypes.create_string_buffer(128)
+    assert L.amss_nccl_unique_id(buf) == 0
+    assert any(buf.raw)
+    H = small_hierarchy()
+    p = D.Plan.of(H, 0, 2, D.partition(H, 2))
+    try:
+        assert L.amss_engine_set_nccl(p._h, buf) < 0
+        assert "commit" in L.amss_last_error().decode()
+    finally:
+        p.close()
