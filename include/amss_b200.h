@@ -293,6 +293,21 @@ int amss_engine_get_level_tiling(amss_engine* e, int level, int* tile_w, int* zs
  * FP32, fewer registers with some spills).  Results do not depend on it. */
 int amss_engine_set_level_occupancy(amss_engine* e, int level, int occ);
 int amss_engine_get_level_occupancy(amss_engine* e, int level, int* occ);
+/* No reference counterpart: the cells a coarse step's final RK4 substep
+ * updates on a level.  In a coarse step (amss_engine_coarse_step and its
+ * graph) every step of a refined level is followed by RestrictProlong
+ * (bssn_class.C:5724-5903), whose prolongation overwrites the level's buffer
+ * cells; the restriction before it reads the new state at most 2 cells past
+ * the physical box (restrict3), and the finer levels' prolongation reads it
+ * around their patches.  Where commit finds every such read within `pad` = 2
+ * cells of the owning block's physical box and every buffer cell prolonged,
+ * the final substep updates only each owned block's cells within that
+ * distance; the other cells' new values would be overwritten unread, so the
+ * coarse step's results are the same bit for bit.  *pad = -1: whole arrays
+ * (level 0, or a hierarchy that fails the test).  A single level step
+ * (amss_engine_step_level) always updates whole arrays.  *points: the cells
+ * the final substep updates on this rank's blocks of the level. */
+int amss_engine_level_final_region(amss_engine* e, int level, int* pad, long long* points);
 
 /* Moving-box regrid (cgh::Regrid_Onelevel, cgh.C:1304-1506, whose data step is
  * cgh::recompose_cgh_Onelevel and Parallel::fill_level_data, Parallel.C).

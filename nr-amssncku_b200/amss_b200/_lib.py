@@ -112,6 +112,7 @@ def lib():
     L.amss_engine_constraint_norms_first_patch.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
     L.amss_engine_set_level_occupancy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.amss_engine_get_level_occupancy.argtypes = [ctypes.c_void_p, ctypes.c_int, _IP]
+    L.amss_engine_level_final_region.argtypes = [ctypes.c_void_p, ctypes.c_int, _IP, ctypes.POINTER(ctypes.c_longlong)]
     L.amss_engine_adm_integrals.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _DP]
     _lib = L
     return L

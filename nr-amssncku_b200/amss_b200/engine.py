@@ -191,6 +191,16 @@ class Engine:
         check(lib().amss_engine_get_level_occupancy(self._h, level, ctypes.byref(o)), "amss_engine_get_level_occupancy")
         return o.value
 
+    def final_region(self, level):
+        """(pad, points) of a level's final substep in a coarse step: pad 2,
+        the owned cells within 2 of the physical box (the rest are overwritten
+        by the prolongation unread); -1, whole arrays.  points: the cells it
+        updates on this engine's blocks."""
+        pad, pts = ctypes.c_int(), ctypes.c_longlong()
+        check(lib().amss_engine_level_final_region(self._h, level, ctypes.byref(pad), ctypes.byref(pts)),
+              "amss_engine_level_final_region")
+        return pad.value, pts.value
+
     def level_tiling(self, level):
         """(tile width as set, z-slabs, stencil work items) of one level."""
         w, z, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -176,6 +176,12 @@ struct StepBlock {
   int lev0;           // 1: Sommerfeld rule on the patch faces; 0: freeze them at u0
   int nf;             // evolved fields: 24 (BSSN) or 25 (Z4c, Theta last)
   int dw;             // stencil-pass tile width (deriv_tile_w of ex[0])
+  int rlo[3], rn[3];  // region of the final substep's region tiles (array indices [rlo, rlo + rn))
 };
+
+// Tile of a pointwise list: tile.x = table index, tile.y = first point.
+// With kRegionTile set in tile.x, the points count the block's final-substep
+// region [rlo, rlo + rn) in x-fastest order instead of its whole array.
+constexpr int kRegionTile = 1 << 30;
 
 }  // namespace amss

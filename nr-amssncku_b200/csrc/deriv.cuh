@@ -73,6 +73,8 @@ struct DerivItem {
   int x0, y0;  // tile origin (array indices)
   int field;
   int k0 = 0, k1 = 0;   // planes [k0, k1) of the march; k1 == 0: the whole block
+  int x1 = 0, y1 = 0;   // columns x < x1, y < y1 only; 0: up to the block's extent
+  int w = 0;            // tile width; 0: the block's (StepBlock::dw)
 };
 
 // kind of a field's stencil record: 0 gradient + Hessian + adv, 1 gradient + adv, 2 adv
@@ -173,17 +175,19 @@ __device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, i
 // of the D array.
 template <typename A, int KIND, typename T, typename S, typename SI>
 __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, const double* bsh,
-                                             int F, int x0, int y0, int k0, int k1, T* D, long long dfs, A* ring) {
+                                             int F, const DerivItem& it, T* D, long long dfs, A* ring) {
   const Coef<A>& C = pick<A>(B.C);
   const int ex0 = B.b.ex[0], ex1 = B.b.ex[1], ex2 = B.b.ex[2];
-  const int kend = k1 > 0 ? k1 : ex2;
+  const int x0 = it.x0, y0 = it.y0, k0 = it.k0;
+  const int kend = it.k1 > 0 ? it.k1 : ex2;
+  const int xend = it.x1 > 0 ? it.x1 : ex0, yend = it.y1 > 0 ? it.y1 : ex1;
   const long long fs = B.b.fs;
-  const int W = B.dw, H = DTHREADS / W;
+  const int W = it.w > 0 ? it.w : B.dw, H = DTHREADS / W;
   const int DSX = W + 6;                     // row stride of the plane buffer
   const int np = DSX * (H + 6);              // cells of one plane (<= DPLANE)
   const int li = threadIdx.x % W, lj = threadIdx.x / W;
   const int i = x0 + li, j = y0 + lj;
-  const bool mine = lj < H && i < ex0 && j < ex1;
+  const bool mine = lj < H && i < xend && j < yend;
   const int fm = B.b.face_mask;
   const bool face_xy = ((fm & 1) && i == ex0 - 1) || ((fm & 2) && j == ex1 - 1) || ((fm & 8) && i == 0) ||
                        ((fm & 16) && j == 0);
@@ -380,16 +384,16 @@ __global__ void __launch_bounds__(DTHREADS, MINB) k_deriv(const StepBlock<T>* __
         // wide fields of the mixed form: FP64 source (state, or the FP64 side stage) and arithmetic
         const double* src = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F) * fs
                                             : (const double*)in + F * fs;
-        deriv_column<double, 0>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<double*>(smem));
+        deriv_column<double, 0>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<double*>(smem));
         __syncthreads();
         continue;
       }
     }
     const SI* src = in + F * fs;
     switch (dkind(F)) {
-      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
-      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
-      default: deriv_column<T, 2>(B, src, in, bsh, F, it.x0, it.y0, it.k0, it.k1, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
+      default: deriv_column<T, 2>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
     }
     __syncthreads();
   }

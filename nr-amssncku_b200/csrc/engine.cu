@@ -128,6 +128,8 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.dtable) cudaFree(L.dtable);
     if (L.dti_tiles) cudaFree(L.dti_tiles);
     if (L.ditems) cudaFree(L.ditems);
+    if (L.dtiles_f) cudaFree(L.dtiles_f);
+    if (L.ditems_f) cudaFree(L.ditems_f);
     if (L.dfaces) cudaFree(L.dfaces);
     if (L.dregion) cudaFree(L.dregion);
     if (L.dregion_first) cudaFree(L.dregion_first);
@@ -263,20 +265,39 @@ static int level_tile_w(const ELevel& L, int ex0) {
 // z extent is cut into L.zsplit slabs of near-equal height (each slab marches
 // its own planes after a 7-plane prologue): more, shorter work items for
 // levels whose items would otherwise fill the last wave of CTAs poorly.
-static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L) {
+// Stencil-pass work items over each owned block's array, or (fin) over its
+// final-substep region: x-y tiles of the level's tile width, z-slabs, ordered by
+// field.
+static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L, bool fin = false) {
   static const int order[25] = {F_CHI, F_LAP, F_BETAX, F_BETAY, F_BETAZ, F_GXX, F_GXY, F_GXZ,
                                 F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
                                 F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
   std::vector<DerivItem> tiles;
   for (size_t m = 0; m < L.own.size(); ++m) {
     const EBlock& b = e->blocks[L.own[m]];
-    const int tw = level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
-    const int ns = std::max(1, std::min(L.zsplit, b.ex[2] / kMinSlab));
+    if (!fin) {
+      const int tw = level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
+      const int ns = std::max(1, std::min(L.zsplit, b.ex[2] / kMinSlab));
+      for (int z = 0; z < ns; ++z) {
+        const int k0 = ns == 1 ? 0 : (int)((long long)b.ex[2] * z / ns);
+        const int k1 = ns == 1 ? 0 : (int)((long long)b.ex[2] * (z + 1) / ns);
+        for (int y0 = 0; y0 < b.ex[1]; y0 += th)
+          for (int x0 = 0; x0 < b.ex[0]; x0 += tw) tiles.push_back(DerivItem{(int)m, x0, y0, 0, k0, k1});
+      }
+      continue;
+    }
+    const Box r = final_region(e, L, b);
+    if (r.empty()) continue;
+    int lo[3], n[3];
+    for (int d = 0; d < 3; ++d) { lo[d] = r.lo[d] - b.org[d]; n[d] = r.hi[d] - r.lo[d]; }
+    // a region narrower than the smallest tile keeps the block's tile, clipped
+    const int tw = n[0] >= kDerivMinEx ? level_tile_w(L, n[0]) : level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
+    const int ns = std::max(1, std::min(L.zsplit, n[2] / kMinSlab));
     for (int z = 0; z < ns; ++z) {
-      const int k0 = ns == 1 ? 0 : (int)((long long)b.ex[2] * z / ns);
-      const int k1 = ns == 1 ? 0 : (int)((long long)b.ex[2] * (z + 1) / ns);
-      for (int y0 = 0; y0 < b.ex[1]; y0 += th)
-        for (int x0 = 0; x0 < b.ex[0]; x0 += tw) tiles.push_back(DerivItem{(int)m, x0, y0, 0, k0, k1});
+      const int k0 = lo[2] + (int)((long long)n[2] * z / ns), k1 = lo[2] + (int)((long long)n[2] * (z + 1) / ns);
+      for (int y0 = lo[1]; y0 < lo[1] + n[1]; y0 += th)
+        for (int x0 = lo[0]; x0 < lo[0] + n[0]; x0 += tw)
+          tiles.push_back(DerivItem{(int)m, x0, y0, 0, k0, k1, lo[0] + n[0], lo[1] + n[1], tw});
     }
   }
   std::vector<DerivItem> items;
@@ -293,7 +314,7 @@ static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L) {
 template <typename T>
 static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<StepBlock<T>> tab;
-  std::vector<int2> tiles;
+  std::vector<int2> tiles, tiles_f;
   std::vector<int2> faces;
   std::vector<DerivItem> items;
   long long doff = 0;
@@ -323,11 +344,20 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     s.lev0 = level == 0 ? 1 : 0;
     s.nf = e->nf;
     s.dw = level_tile_w(L, b.ex[0]);
+    const Box fr = final_region(e, L, b);
+    for (int d = 0; d < 3; ++d) {
+      s.rlo[d] = fr.lo[d] - b.org[d];
+      s.rn[d] = fr.empty() ? 0 : fr.hi[d] - fr.lo[d];
+    }
     if (b.lowsym) L.symm = true;
     tab.push_back(s);
     // substep tiles: kPointwiseTile points for the split form's pointwise pass, 128 for the fused kernel
     const long long tstep = e->prm.kernel == 0 ? kPointwiseTile : 128;
     for (long long p = 0; p < b.npts; p += tstep) tiles.push_back(make_int2((int)m, (int)p));
+    if (L.final_pad >= 0) {
+      const long long nr = (long long)s.rn[0] * s.rn[1] * s.rn[2];
+      for (long long q = 0; q < nr; q += tstep) tiles_f.push_back(make_int2((int)m | kRegionTile, (int)q));
+    }
     if (b.face_mask) {
       const int fm = b.face_mask;
       for (int k = 0; k < b.ex[2]; ++k)
@@ -341,7 +371,10 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     }
   }
   items = deriv_items(e, L);
+  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, true) : std::vector<DerivItem>();
   L.ntiles = (int)tiles.size();
+  L.ntiles_f = (int)tiles_f.size();
+  L.nditems_f = (int)items_f.size();
   {
     // constraint-norm region of each table block, in array indices.  A block
     // added by bbox: 3 ghost cells off each side, unless the side's outer cell
@@ -401,6 +434,14 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   }
   AMSS_CK(cudaMalloc(&L.dtiles, tiles.size() * sizeof(int2)));
   AMSS_CK(cudaMemcpy(L.dtiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  if (!tiles_f.empty()) {
+    AMSS_CK(cudaMalloc(&L.dtiles_f, tiles_f.size() * sizeof(int2)));
+    AMSS_CK(cudaMemcpy(L.dtiles_f, tiles_f.data(), tiles_f.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
+  if (!items_f.empty()) {
+    AMSS_CK(cudaMalloc(&L.ditems_f, items_f.size() * sizeof(DerivItem)));
+    AMSS_CK(cudaMemcpy(L.ditems_f, items_f.data(), items_f.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  }
   return 0;
 }
 
@@ -455,6 +496,7 @@ extern "C" int amss_engine_commit(amss_engine* e) {
   int nlev = 0;
   if (int rc = prepare_levels(e, &nlev)) return rc;
   if (int rc = build_xfers(e)) return rc;
+  plan_final_regions(e);
   // arrays of the blocks this rank owns; the others are geometry only
   size_t bytes = 0;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -551,6 +593,7 @@ extern "C" int amss_plan_commit(amss_engine* e) {
   int nlev = 0;
   if (int rc = prepare_levels(e, &nlev)) return rc;
   if (int rc = build_xfers(e)) return rc;
+  plan_final_regions(e);
   e->committed = true;
   return 0;
 }
@@ -675,7 +718,9 @@ static int sync_level(amss_engine* e, ELevel& L, int which) { return run_xfer(e,
 
 // One RK4 step of every block of a level (bssn_class::Step, bssn_class.C:2981-3915):
 // four fused substep launches, a ghost sync after each, the ring rotation.
-static int step_level_impl(amss_engine* e, int level, double dt) {
+// fin: the step is one of a coarse step, so RestrictProlong follows and the
+// final substep may take the level's final-substep regions.
+static int step_level_impl(amss_engine* e, int level, double dt, bool fin = false) {
   auto it = e->levels.find(level);
   if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_step_level: no such level");
   ELevel& L = it->second;
@@ -685,7 +730,6 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
   rk.sixth_dt = (1.0 / 6.0) * dt;
   rk.chitiny = e->prm.chitiny;
   const bool mixed = e->prm.precision == 1;
-  const int grid = std::min(L.ntiles, e->sm_count * 8);
   // a rank without blocks on this level still takes part in its transfers
   const bool work = !L.own.empty();
   // enforce_ga on U0 in place (bssn_class.C:3052); the stage outputs of
@@ -696,9 +740,16 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
     e->launches++;
   }
   const bool split = e->prm.kernel == 0;
-  const int dgrid = std::min(L.nditems, e->sm_count * 16);
   const bool track = e->ntrack > 0 && level == e->track_level;
   for (int sub = 0; sub < 4; ++sub) {
+    // the final substep over the regions, where the level has them
+    const bool reg = fin && sub == 3 && L.final_pad >= 0;
+    const DerivItem* ditems = reg ? L.ditems_f : L.ditems;
+    const int nditems = reg ? L.nditems_f : L.nditems;
+    const int2* tiles = reg ? L.dtiles_f : L.dtiles;
+    const int ntiles = reg ? L.ntiles_f : L.ntiles;
+    const int dgrid = std::min(nditems, e->sm_count * 16);
+    const int grid = std::min(ntiles, e->sm_count * 8);
     if (!work) {
       if (sub < 3)
         if (int rc = sync_level(e, L, sub == 1 ? BUF_STAGE_B : BUF_STAGE_A)) return rc;
@@ -711,16 +762,18 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
                            e->prm.symmetry, e->stream));
       e->launches++;
     }
-    if (split) {
+    if (split && nditems) {
       const cudaError_t ed =
-          mixed ? launch_deriv<float, float>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc)
-                : launch_deriv<double, double>(L.dtable, L.ditems, L.nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc);
+          mixed ? launch_deriv<float, float>(L.dtable, ditems, nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc)
+                : launch_deriv<double, double>(L.dtable, ditems, nditems, sub, e->D, L.dfs, dgrid, e->stream, L.docc);
       AMSS_CK(ed);
       e->launches++;
     }
 #define AMSS_SUB(T, SY, SP, Z) \
-    launch_substep<T, T, SY, SP, Z>(L.dtable, L.dtiles, L.ntiles, sub, rk, enf, e->dstatus, grid, e->stream, e->D, L.dfs)
-    if (e->nf == NFIELDS_Z4C)   // split form only (checked at create)
+    launch_substep<T, T, SY, SP, Z>(L.dtable, tiles, ntiles, sub, rk, enf, e->dstatus, grid, e->stream, e->D, L.dfs)
+    if (ntiles == 0)
+      err = cudaSuccess;
+    else if (e->nf == NFIELDS_Z4C)   // split form only (checked at create)
       err = mixed ? (L.symm ? AMSS_SUB(float, true, true, true) : AMSS_SUB(float, false, true, true))
                   : (L.symm ? AMSS_SUB(double, true, true, true) : AMSS_SUB(double, false, true, true));
     else if (mixed)
@@ -731,7 +784,7 @@ static int step_level_impl(amss_engine* e, int level, double dt) {
                   : (L.symm ? AMSS_SUB(double, true, false, false) : AMSS_SUB(double, false, false, false));
 #undef AMSS_SUB
     AMSS_CK(err);
-    e->launches++;
+    if (ntiles) e->launches++;
     if (L.nfaces) {
       const cudaError_t ef =
           mixed ? (L.symm ? launch_face<float, float, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
@@ -775,7 +828,7 @@ static int recursive_step(amss_engine* e, int l, double dt0) {
   const double dt = dt0 / std::ldexp(1.0, l);
   for (int i = 0; i < iters; ++i) {
     const bool yn = i == iters - 1;
-    if (int rc = step_level_impl(e, l, dt)) return rc;
+    if (int rc = step_level_impl(e, l, dt, true)) return rc;
     if (l < nlev - 1)
       if (int rc = recursive_step(e, l + 1, dt0)) return rc;
     if (l > 0)
@@ -806,13 +859,37 @@ extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_
   L.tile_w = tile_w;
   L.zsplit = zsplit;
   const std::vector<DerivItem> items = deriv_items(e, L);
+  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, true) : std::vector<DerivItem>();
   if (L.ditems) cudaFree(L.ditems);
-  L.ditems = nullptr;
+  if (L.ditems_f) cudaFree(L.ditems_f);
+  L.ditems = L.ditems_f = nullptr;
   L.nditems = (int)items.size();
+  L.nditems_f = (int)items_f.size();
   if (items.empty()) return 0;
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  if (!items_f.empty()) {
+    AMSS_CK(cudaMalloc(&L.ditems_f, items_f.size() * sizeof(DerivItem)));
+    AMSS_CK(cudaMemcpy(L.ditems_f, items_f.data(), items_f.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  }
   return e->prm.precision == 1 ? patch_table_dw<float>(e, L) : patch_table_dw<double>(e, L);
+}
+
+extern "C" int amss_engine_level_final_region(amss_engine* e, int level, int* pad, long long* points) {
+  if (!e || !e->committed) return amss_fail(AMSS_ERR_STATE, "engine not committed");
+  auto it = e->levels.find(level);
+  if (it == e->levels.end()) return amss_fail(AMSS_ERR_ARG, "amss_engine_level_final_region: no such level");
+  const ELevel& L = it->second;
+  if (pad) *pad = L.final_pad;
+  if (points) {
+    long long n = 0;
+    for (int b : L.own) {
+      const Box r = final_region(e, L, e->blocks[b]);
+      if (!r.empty()) n += (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
+    }
+    *points = n;
+  }
+  return 0;
 }
 
 extern "C" int amss_engine_set_level_occupancy(amss_engine* e, int level, int occ) {

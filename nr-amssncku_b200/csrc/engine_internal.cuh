@@ -120,6 +120,15 @@ struct ELevel {
   int nfaces = 0;
   DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
   int nditems = 0;
+  // The final substep of a coarse step's level step over each block's owned
+  // cells within final_pad of its patch's physical box (-1: whole arrays):
+  // the cells further out are overwritten by the prolongation into the
+  // level's buffer before anything reads them (plan_final_regions).
+  int final_pad = -1;
+  int2* dtiles_f = nullptr;     // region tiles of the final substep's pointwise pass
+  int ntiles_f = 0;
+  DerivItem* ditems_f = nullptr;   // and its stencil-pass items
+  int nditems_f = 0;
   int tile_w = 0;               // stencil-pass tile width (0: deriv_tile_w of each block's x extent)
   int zsplit = 1;               // z-slabs per block in the stencil pass
   int docc = 0;                 // stencil-pass occupancy form: 0 two resident CTAs, 1 more (deriv.cuh)
@@ -188,5 +197,9 @@ int run_xfer(amss_engine* e, int op, int arg);        // arg: sync buffer, restr
 void release_xfers(amss_engine* e);
 void amss_xfer_detach(amss_engine* e);              // leaves its group, destroys its NCCL communicator
 int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf = 0);
+// Sets each level's final_pad where the final-substep regions are safe.
+void plan_final_regions(amss_engine* e);
+// The final-substep region of a block (global level indices; empty: none).
+Box final_region(const amss_engine* e, const ELevel& L, const EBlock& b);
 void push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b);
 }  // namespace amss

@@ -16,6 +16,24 @@
 
 namespace amss {
 
+// Points of a tile list's range in a block: its array, or its region.
+template <typename T>
+__device__ __forceinline__ long long tile_count(const StepBlock<T>& B, bool region) {
+  return region ? (long long)B.rn[0] * B.rn[1] * B.rn[2] : B.npts;
+}
+
+// Array point of entry q of a tile's point range, or -1 past its end.
+template <typename T>
+__device__ __forceinline__ long long tile_point(const StepBlock<T>& B, bool region, long long q) {
+  if (q >= tile_count(B, region)) return -1;
+  if (!region) return q;
+  const long long n01 = (long long)B.rn[0] * B.rn[1];
+  const int k = (int)(q / n01);
+  const long long r = q - (long long)k * n01;
+  const int j = (int)(r / B.rn[0]), i = (int)(r - (long long)j * B.rn[0]);
+  return (long long)(i + B.rlo[0]) + (long long)B.b.ex[0] * ((long long)(j + B.rlo[1]) + (long long)B.b.ex[1] * (k + B.rlo[2]));
+}
+
 // Fused RK4 substep over a tile list of one level.  Substep `sub` reads
 // (sub0: u0, sub1: A, sub2: B, sub3: A) and writes (A, B, A, unew).
 // SPLIT: the stencil terms come from the D array the stencil pass (k_deriv)
@@ -28,7 +46,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
                                                                     long long dfs) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
-    const StepBlock<T>& B = blocks[tile.x];
+    const bool region = (tile.x & kRegionTile) != 0;
+    const StepBlock<T>& B = blocks[tile.x & ~kRegionTile];
 #if AMSS_POINTWISE_PREFETCH
     // split form: pull the rows of a tile (D slots, stage input, u0, K) into
     // L2 -- the next tile's while this one computes, or this tile's before its
@@ -42,13 +61,19 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
       const int tn = pass == 0 ? t : t + (int)gridDim.x;
       if (threadIdx.x < 32 && tn < ntiles) {
         const int2 nt = tiles[tn];
-        const StepBlock<T>& N = blocks[nt.x];
-        const long long fs = N.b.fs, q0 = nt.y;
+        const bool nreg = (nt.x & kRegionTile) != 0;
+        const StepBlock<T>& N = blocks[nt.x & ~kRegionTile];
+        const long long fs = N.b.fs;
         const int cur = N.lvl[0];
         const SI* nin = sub == 0 ? (const SI*)N.tl[cur] : (const SI*)N.stage[sub == 2 ? 1 : 0];
-        // the tile's points only (the last tile of a block is short), rounded up to
-        // 16 bytes: still inside the block's field, whose stride is a multiple of 64
-        const long long nel = N.npts - q0 < 128 ? N.npts - q0 : 128;
+        // the array span of the tile's points (the last tile of a block is short; a
+        // region tile's rows are strided, the span holds them), at most two tiles'
+        // worth, rounded up to 16 bytes: still inside the block's field, whose
+        // stride is a multiple of 64
+        const long long cnt = tile_count(N, nreg);
+        const long long pl = tile_point(N, nreg, (long long)nt.y + 127 < cnt ? (long long)nt.y + 127 : cnt - 1);
+        const long long q0 = tile_point(N, nreg, nt.y);
+        const long long nel = pl - q0 + 1 < 2 * 128 ? pl - q0 + 1 : 2 * 128;
         for (int r = threadIdx.x; r < D_SLOTS + 72; r += 32) {
           const char* a;
           int es;
@@ -67,8 +92,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
      }
     }
 #endif
-    const long long p = (long long)tile.y + threadIdx.x;
-    if (p >= B.npts) continue;
+    const long long p = tile_point(B, region, (long long)tile.y + threadIdx.x);
+    if (p < 0) continue;
     const int cur = B.lvl[0];
     double* u0 = B.tl[cur];
     const SI* in = sub == 0 ? (const SI*)u0 : (const SI*)B.stage[sub == 2 ? 1 : 0];

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -183,6 +184,96 @@ static int plan_xfer(amss_engine* e, int kind, int level, const std::vector<AmrB
   }
   e->xfers.push_back(std::move(op));
   return (int)e->xfers.size() - 1;
+}
+
+// ---- final-substep regions ---------------------------------------------------
+// In a coarse step every level step of a refined level is followed by its
+// RestrictProlong (bssn_class.C:5724-5903): the restriction reads the level's
+// new state around its physical boxes, then the prolongation overwrites the
+// level's buffer cells.  In between, only the finer levels' prolongation reads
+// the level (its new state, or the time interpolation formed from it).  Where
+// each of these reads, and every physical cell, stays within kFinalPad cells
+// of the physical box of the block that owns the cell, and the prolongation
+// covers every buffer cell of the level's arrays, the final RK4 substep need
+// not update the owned cells further out: nothing reads their new values
+// before the prolongation replaces them.  The state after the coarse step is
+// the same bit for bit.
+static const int kFinalPad = 2;   // restrict3 reads fine cells 2k-2 .. 2k+3
+
+static Box grow(const Box& b, int g) {
+  Box r = b;
+  for (int d = 0; d < 3; ++d) { r.lo[d] -= g; r.hi[d] += g; }
+  return r;
+}
+static long long volume(const Box& b) {
+  return b.empty() ? 0 : (long long)(b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]) * (b.hi[2] - b.lo[2]);
+}
+
+// Every cell of R is owned by a block of L within pad of its patch's physical box.
+static bool reads_valid(const amss_engine* e, const ELevel& L, const Box& R, int pad) {
+  long long cov = 0;
+  for (int y : L.blocks) {
+    const EBlock& Y = e->blocks[y];
+    const Box s = intersect(R, Y.own);
+    if (s.empty()) continue;
+    const Box ok = intersect(s, grow(e->patches[Y.patch].phys, pad));
+    if (volume(ok) != volume(s)) return false;
+    cov += volume(s);
+  }
+  return cov == volume(R);
+}
+
+Box final_region(const amss_engine* e, const ELevel& L, const EBlock& b) {
+  if (L.final_pad < 0 || b.patch < 0) return b.array();
+  return intersect(intersect(b.own, grow(e->patches[b.patch].phys, L.final_pad)), b.array());
+}
+
+void plan_final_regions(amss_engine* e) {
+  for (auto& kv : e->levels) kv.second.final_pad = -1;
+  for (auto& kv : e->levels) {
+    const int l = kv.first;
+    ELevel& L = kv.second;
+    if (l == 0 || L.blocks.empty() || !e->levels.count(l - 1)) continue;
+    const ELevel& C = e->levels.at(l - 1);
+    bool ok = true;
+    // blocks of buffered patches, owned boxes disjoint
+    for (size_t a = 0; a < L.blocks.size() && ok; ++a) {
+      const EBlock& A = e->blocks[L.blocks[a]];
+      if (A.patch < 0 || e->patches[A.patch].buffer <= 0) ok = false;
+      for (size_t b = a + 1; b < L.blocks.size() && ok; ++b)
+        if (volume(intersect(A.own, e->blocks[L.blocks[b]].own)) != 0) ok = false;
+    }
+    if (!ok) continue;
+    // the prolongation into the level writes every array cell outside the
+    // physical box; the physical cells are valid
+    std::map<int, long long> cover;
+    for (const AmrBox& b : prolong_boxes(e, L, C)) cover[b.dst] += (long long)b.n[0] * b.n[1] * b.n[2];
+    for (int x : L.blocks) {
+      const EBlock& X = e->blocks[x];
+      const Box ph = intersect(X.array(), e->patches[X.patch].phys);
+      if (cover[x] != volume(X.array()) - volume(ph) || !reads_valid(e, L, ph, kFinalPad)) { ok = false; break; }
+    }
+    // the restriction out of the level: fine 2k-2 .. 2k+3 of coarse cell k
+    if (ok)
+      for (const AmrBox& b : restrict_boxes(e, L, C)) {
+        Box R;
+        for (int d = 0; d < 3; ++d) { R.lo[d] = 2 * b.lo[d] - 2; R.hi[d] = 2 * (b.lo[d] + b.n[d]) + 2; }
+        if (!reads_valid(e, L, R, kFinalPad)) { ok = false; break; }
+      }
+    // the prolongation into the next finer level: coarse (g >> 1) - 3 .. + 2 of
+    // an even fine cell g, (g >> 1) - 2 .. + 3 of an odd one
+    if (ok && e->levels.count(l + 1))
+      for (const AmrBox& b : prolong_boxes(e, e->levels.at(l + 1), L)) {
+        Box R;
+        for (int d = 0; d < 3; ++d) {
+          const int g0 = b.lo[d], g1 = b.lo[d] + b.n[d] - 1;
+          R.lo[d] = (g0 & 1) ? (g0 >> 1) - 2 : (g0 >> 1) - 3;
+          R.hi[d] = ((g1 & 1) ? (g1 >> 1) - 2 : (g1 >> 1) - 3) + 6;
+        }
+        if (!reads_valid(e, L, R, kFinalPad)) { ok = false; break; }
+      }
+    if (ok) L.final_pad = kFinalPad;
+  }
 }
 
 int build_xfers(amss_engine* e) {

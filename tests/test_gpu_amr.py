@@ -373,3 +373,60 @@ def test_puncture_tracking_mixed():
     got = e.punctures()
     e.close()
     assert np.abs(got - np.array(oh.porg0)).max() <= 1e-9
+
+
+def test_final_substep_regions_in_use():
+    """The coarse-step parity above runs with final-substep regions on both
+    refined levels (the owned cells within 2 of the physical box)."""
+    H = small_hierarchy()
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
+    try:
+        assert e.final_region(0) == (-1, H.points(0))
+        for lv in (1, 2):
+            pad, pts = e.final_region(lv)
+            assert pad == 2 and 0 < pts < H.points(lv)
+    finally:
+        e.close()
+
+
+def test_single_level_step_updates_every_cell(fp64_reference):
+    """amss_engine_step_level is not followed by RestrictProlong: its final
+    substep still updates the buffer cells, as the oracle's level step does."""
+    H, init, dt0, _ = fp64_reference
+    oh = OA.OracleHierarchy(H, eps=0.1)
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
+    try:
+        for i, st in enumerate(init):
+            oh.set_state(i, st)
+            e.set_state(i, st)
+        dt = dt0 / 2
+        assert oh.level_step(1, dt) == 0
+        e.step(1, dt)
+        assert e.sync() == 0
+        ids = [i for p in H.levels[1] for i in p.blocks]
+        errs = _errs([e.get_state(i) for i in ids], [oh.state(i) for i in ids])
+        assert errs.max() <= 1e-12, errs
+    finally:
+        e.close()
+
+
+def test_level_without_regions_matches_oracle():
+    """Level 2's buffered box reaches level 1's physical boundary: level 1
+    keeps whole arrays in its final substep, level 2 takes regions; two
+    coarse steps against the oracle."""
+    from amss_b200.hierarchy import Hierarchy
+    H = Hierarchy(-8.0, 0.5)
+    H.add_patch(0, (0, 0, 0), (32, 32, 32), 0, [[], [], []])
+    H.add_patch(1, (24, 24, 24), (40, 40, 40), 6, [[32], [], []])
+    H.add_patch(2, (54, 54, 54), (70, 70, 70), 6, [[], [62], []])
+    init = OA.initial_state(H, [0.5], [[0.1, 0.05, 0.02]], noise=1e-8)
+    dt0 = 0.25 * H.h0
+    ref = _run_oracle(H, init, dt0, 2)
+    e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
+    try:
+        assert e.final_region(1)[0] == -1 and e.final_region(2)[0] == 2
+    finally:
+        e.close()
+    got = _run_engine(H, init, dt0, 2)
+    errs = _errs(got, ref)
+    assert errs.max() <= 1e-12, errs
