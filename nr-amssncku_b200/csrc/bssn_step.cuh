@@ -87,7 +87,10 @@ struct EpiRK {
     const double k = (double)kv;
     const double u = u0[o];
     double r;
-    if (sub == 0) {
+    if (freeze) {
+      // a frozen point's accumulator is never read (it would only feed r)
+      r = u;
+    } else if (sub == 0) {
       r = u + c.half_dt * k;
       K[o] = k;
     } else if (sub == 1) {
@@ -99,7 +102,6 @@ struct EpiRK {
     } else {
       r = u + c.sixth_dt * (k + K[o]);
     }
-    if (freeze) r = u;
     if constexpr (F == F_CHI) {
       if (r < c.chitiny) r = c.chitiny;
     }

@@ -785,7 +785,8 @@ static int step_level_impl(amss_engine* e, int level, double dt, bool fin = fals
 #undef AMSS_SUB
     AMSS_CK(err);
     if (ntiles) e->launches++;
-    if (L.nfaces) {
+    // refined-patch faces are frozen cells past the final substep's regions
+    if (L.nfaces && !reg) {
       const cudaError_t ef =
           mixed ? (L.symm ? launch_face<float, float, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
                           : launch_face<float, float, false>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream))
