@@ -785,15 +785,28 @@ static int step_level_impl(amss_engine* e, int level, double dt, bool fin = fals
 #undef AMSS_SUB
     AMSS_CK(err);
     if (ntiles) e->launches++;
-    // refined-patch faces are frozen cells past the final substep's regions
-    if (L.nfaces && !reg) {
-      const cudaError_t ef =
-          mixed ? (L.symm ? launch_face<float, float, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
-                          : launch_face<float, float, false>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream))
-                : (L.symm ? launch_face<double, double, true>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream)
-                          : launch_face<double, double, false>(L.dtable, L.dfaces, L.nfaces, sub, rk, enf, e->dstatus, e->stream));
-      AMSS_CK(ef);
+    // Outer faces.  Level 0: the Sommerfeld rule at every substep.  A refined
+    // level's faces are frozen at U0 (enforced in substeps 0-2): the same
+    // values in stage A at substeps 0 and 2 and in stage B at substep 1, so
+    // substep 0 writes both stages and substeps 1 and 2 launch nothing; the
+    // final substep writes the frozen new state unless the level takes
+    // regions, past which the faces lie.
+    auto face = [&](int s) -> cudaError_t {
       e->launches++;
+      return mixed ? (L.symm ? launch_face<float, float, true>(L.dtable, L.dfaces, L.nfaces, s, rk, enf, e->dstatus, e->stream)
+                             : launch_face<float, float, false>(L.dtable, L.dfaces, L.nfaces, s, rk, enf, e->dstatus, e->stream))
+                   : (L.symm ? launch_face<double, double, true>(L.dtable, L.dfaces, L.nfaces, s, rk, enf, e->dstatus, e->stream)
+                             : launch_face<double, double, false>(L.dtable, L.dfaces, L.nfaces, s, rk, enf, e->dstatus, e->stream));
+    };
+    if (L.nfaces) {
+      if (level == 0) {
+        AMSS_CK(face(sub));
+      } else if (sub == 0) {
+        AMSS_CK(face(0));
+        AMSS_CK(face(1));
+      } else if (sub == 3 && !reg) {
+        AMSS_CK(face(3));
+      }
     }
     if (sub < 3) {
       if (int rc = sync_level(e, L, sub == 1 ? BUF_STAGE_B : BUF_STAGE_A)) return rc;
