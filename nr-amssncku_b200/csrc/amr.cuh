@@ -149,18 +149,20 @@ __global__ void k_amr_prolong(const AmrBlock* __restrict__ blocks, const AmrBox*
 // Coarse cells of dst (coarse) from fine src: restrict3
 // (prolongrestrict_cell.f90:2330-2468): fine 2k-2..2k+3 with weights
 // C1 C2 C3 C3 C2 C1, z then y then x.  Writes the current state or the
-// time-interpolated temp.
+// time-interpolated temp.  One thread per (field, coarse cell) unit,
+// field-major within a box, so consecutive threads take consecutive cells.
 __global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
                                const int2* __restrict__ tiles, int ntiles, int to_temp, unsigned* status) {
   const double C1 = 3.0 / 2.56e2, C2 = -2.5e1 / 2.56e2, C3 = 7.5e1 / 1.28e2;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
     const AmrBox& bx = boxes[tile.x];
-    const int p = tile.y + threadIdx.x;
-    const int np = bx.n[0] * bx.n[1] * bx.n[2];
-    if (p >= np) continue;
-    const int c[3] = {bx.lo[0] + p % bx.n[0], bx.lo[1] + (p / bx.n[0]) % bx.n[1], bx.lo[2] + p / (bx.n[0] * bx.n[1])};
     const AmrBlock& D = blocks[bx.dst];
+    const int np = bx.n[0] * bx.n[1] * bx.n[2];
+    const int uu = tile.y + threadIdx.x;
+    if (uu >= np * D.nf) continue;
+    const int f = uu / np, p = uu - f * np;
+    const int c[3] = {bx.lo[0] + p % bx.n[0], bx.lo[1] + (p / bx.n[0]) % bx.n[1], bx.lo[2] + p / (bx.n[0] * bx.n[1])};
     const AmrBlock& S = blocks[bx.src];
     const int f0[3] = {2 * c[0] - 2, 2 * c[1] - 2, 2 * c[2] - 2};
     if (!amr_inside(D, c[0], c[1], c[2]) || !amr_inside(S, f0[0], f0[1], f0[2]) ||
@@ -168,33 +170,26 @@ __global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox
       atomicOr(status, ST_BAD_ARG);
       continue;
     }
-    const double* src = amr_state(S);
     const long long sy = S.ex[0], sz = (long long)S.ex[0] * S.ex[1];
-    const long long base = amr_idx(S, f0[0], f0[1], f0[2]);
-    double out[NFIELDS_Z4C];
-    for (int f = 0; f < D.nf; ++f) {
-      const double* q = src + f * S.fs + base;
-      double tmp1[6];
-      for (int a = 0; a < 6; ++a) {
-        double t2[6];
-        for (int b = 0; b < 6; ++b) {
-          const double* r = q + a + b * sy;
-          t2[b] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(r[0], r[5 * sz])), __dmul_rn(C2, __dadd_rn(r[sz], r[4 * sz]))),
-                            __dmul_rn(C3, __dadd_rn(r[2 * sz], r[3 * sz])));
-        }
-        tmp1[a] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(t2[0], t2[5])), __dmul_rn(C2, __dadd_rn(t2[1], t2[4]))),
-                            __dmul_rn(C3, __dadd_rn(t2[2], t2[3])));
+    const double* q = amr_state(S) + f * S.fs + amr_idx(S, f0[0], f0[1], f0[2]);
+    double tmp1[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      double t2[6];
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        const double* r = q + a + b * sy;
+        t2[b] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(r[0], r[5 * sz])), __dmul_rn(C2, __dadd_rn(r[sz], r[4 * sz]))),
+                          __dmul_rn(C3, __dadd_rn(r[2 * sz], r[3 * sz])));
       }
-      out[f] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(tmp1[0], tmp1[5])), __dmul_rn(C2, __dadd_rn(tmp1[1], tmp1[4]))),
-                         __dmul_rn(C3, __dadd_rn(tmp1[2], tmp1[3])));
+      tmp1[a] = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(t2[0], t2[5])), __dmul_rn(C2, __dadd_rn(t2[1], t2[4]))),
+                          __dmul_rn(C3, __dadd_rn(t2[2], t2[3])));
     }
-    const long long od = amr_idx(D, c[0], c[1], c[2]);
-    if (to_temp) {
-      for (int f = 0; f < D.nf; ++f) D.K[f * D.fs + od] = out[f];
-    } else {
-      double* dst = amr_state(D);
-      for (int f = 0; f < D.nf; ++f) dst[f * D.fs + od] = out[f];
-    }
+    const double v = __dadd_rn(__dadd_rn(__dmul_rn(C1, __dadd_rn(tmp1[0], tmp1[5])), __dmul_rn(C2, __dadd_rn(tmp1[1], tmp1[4]))),
+                               __dmul_rn(C3, __dadd_rn(tmp1[2], tmp1[3])));
+    const long long od = (long long)f * D.fs + amr_idx(D, c[0], c[1], c[2]);
+    if (to_temp) D.K[od] = v;
+    else amr_state(D)[od] = v;
   }
 }
 

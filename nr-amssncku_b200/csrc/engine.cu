@@ -445,13 +445,14 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   return 0;
 }
 
-// Tiles of 128 work units per box: box cells, or (prolong_nf fields) the
-// (field, run of kProlongRun fine cells along x) units the prolongation counts.
-int amss::upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf) {
+// Tiles of 128 work units per box: box cells; with nf fields, the (field,
+// cell) units the restriction counts, or (runs) the (field, run of
+// kProlongRun fine cells along x) units the prolongation counts.
+int amss::upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int nf, bool runs) {
   std::vector<int2> tiles;
   for (size_t m = 0; m < boxes.size(); ++m) {
-    const long long nx = prolong_nf ? prolong_runs_x(boxes[m].lo[0], boxes[m].n[0]) : boxes[m].n[0];
-    const long long n = nx * boxes[m].n[1] * boxes[m].n[2] * (prolong_nf ? prolong_nf : 1);
+    const long long nx = runs ? prolong_runs_x(boxes[m].lo[0], boxes[m].n[0]) : boxes[m].n[0];
+    const long long n = nx * boxes[m].n[1] * boxes[m].n[2] * (nf ? nf : 1);
     for (long long p = 0; p < n; p += 128) tiles.push_back(make_int2((int)m, (int)p));
   }
   D.ntiles = (int)tiles.size();
@@ -1026,7 +1027,7 @@ extern "C" int amss_engine_regrid_fill(amss_engine* dst, amss_engine* src, int l
   AMSS_CK(cudaMalloc(&dtab, tab.size() * sizeof(AmrBlock)));
   AMSS_CK(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(AmrBlock), cudaMemcpyHostToDevice));
   AMSS_CK(cudaMemsetAsync(dst->dstatus, 0, sizeof(unsigned), dst->stream));
-  if ((rc = upload_boxes(cp, dcp)) == 0 && (rc = upload_boxes(pr, dpr, dst->nf)) == 0) {
+  if ((rc = upload_boxes(cp, dcp)) == 0 && (rc = upload_boxes(pr, dpr, dst->nf, true)) == 0) {
     cudaError_t err = cudaSuccess;
     if (dcp.ntiles)
       err = launch_amr_sync(dtab, dcp.boxes, dcp.tiles, dcp.ntiles, BUF_STATE, dst->prm.precision == 1, dst->dstatus,

@@ -196,7 +196,7 @@ int upload_xfers(amss_engine* e, std::vector<AmrBlock>& table);   // staging are
 int run_xfer(amss_engine* e, int op, int arg);        // arg: sync buffer, restrict to_temp, prolong from_temp
 void release_xfers(amss_engine* e);
 void amss_xfer_detach(amss_engine* e);              // leaves its group, destroys its NCCL communicator
-int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int prolong_nf = 0);
+int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int nf = 0, bool runs = false);
 // Sets each level's final_pad where the final-substep regions are safe.
 void plan_final_regions(amss_engine* e);
 // The final-substep region of a block (global level indices; empty: none).

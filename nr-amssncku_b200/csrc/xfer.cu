@@ -315,7 +315,7 @@ int upload_xfers(amss_engine* e, std::vector<AmrBlock>& table) {
     table.push_back(a);
   }
   for (XferOp& op : e->xfers) {
-    if (int rc = upload_boxes(op.run_h, op.run, op.kind == XF_PROLONG ? e->nf : 0)) return rc;
+    if (int rc = upload_boxes(op.run_h, op.run, op.kind == XF_SYNC ? 0 : e->nf, op.kind == XF_PROLONG)) return rc;
     if (int rc = upload_boxes(op.unpack_h, op.unpack)) return rc;
   }
   return 0;
