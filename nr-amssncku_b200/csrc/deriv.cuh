@@ -82,6 +82,18 @@ __host__ __device__ constexpr int dkind(int F) { return dslots(F) == 10 ? 0 : (d
 
 __device__ __forceinline__ int ring_slot(int m) { return (m + 3) % DRING; }   // m >= -3
 
+// A stencil term into D: written once here and read once by the pointwise
+// pass, so with AMSS_D_STREAMING bit 0 the store is marked evict-first
+// (st.global.cs) and leaves L2 to the fields the stencil pass re-reads.
+template <typename T>
+__device__ __forceinline__ void dstore(T* a, T v) {
+#if AMSS_D_STREAMING & 1
+  __stcs(a, v);
+#else
+  *a = v;
+#endif
+}
+
 // The plane cells one thread fills, with their in-plane offsets and the x/y
 // mirror signs, fixed for the whole march.
 template <typename A, typename S>
@@ -286,9 +298,9 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
           else { gx = dx2(qk); gy = dy2(qk); }
           gz = C.d2[2] * (-Z(-1) + Z(1));
         }
-        d[(o + 0) * dfs + p] = (T)gx;
-        d[(o + 1) * dfs + p] = (T)gy;
-        d[(o + 2) * dfs + p] = (T)gz;
+        dstore(d + (o + 0) * dfs + p, (T)gx);
+        dstore(d + (o + 1) * dfs + p, (T)gy);
+        dstore(d + (o + 2) * dfs + p, (T)gz);
       }
       if constexpr (KIND == 0) {
         A hxx = A(0), hxy = A(0), hxz = A(0), hyy = A(0), hyz = A(0), hzz = A(0);
@@ -312,12 +324,12 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
           hxz = C.d2[2] * (-fx2[0] + fx2[2]);
           hyz = C.d2[2] * (-fy2[0] + fy2[2]);
         }
-        d[(o + 3) * dfs + p] = (T)hxx;
-        d[(o + 4) * dfs + p] = (T)hxy;
-        d[(o + 5) * dfs + p] = (T)hxz;
-        d[(o + 6) * dfs + p] = (T)hyy;
-        d[(o + 7) * dfs + p] = (T)hyz;
-        d[(o + 8) * dfs + p] = (T)hzz;
+        dstore(d + (o + 3) * dfs + p, (T)hxx);
+        dstore(d + (o + 4) * dfs + p, (T)hxy);
+        dstore(d + (o + 5) * dfs + p, (T)hxz);
+        dstore(d + (o + 6) * dfs + p, (T)hyy);
+        dstore(d + (o + 7) * dfs + p, (T)hyz);
+        dstore(d + (o + 8) * dfs + p, (T)hzz);
       }
       A adv = A(0);
       if (G.lop) {
@@ -346,7 +358,7 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
                kodiv(ko_sum_rn<A, false>(Z), C, 2);
         adv = adv + C.ko * ks;
       }
-      d[(o + dslots(F) - 1) * dfs + p] = (T)adv;
+      dstore(d + (o + dslots(F) - 1) * dfs + p, (T)adv);
     }
     // slide the register windows
 #pragma unroll

@@ -133,6 +133,10 @@ static_assert(doff(24) == D_SLOTS, "D slot layout");
 constexpr int D_SLOTS_Z4C = D_SLOTS + 4;
 static_assert(doff(F_TZ) == D_SLOTS && doff(F_TZ + 1) == D_SLOTS_Z4C, "Z4c D slot layout");
 
+#ifndef AMSS_D_STREAMING   // the D array marked evict-first: bit 0 its stores, bit 1 its loads
+#define AMSS_D_STREAMING 0
+#endif
+
 // Accessor of the pointwise pass: centre values from the stage input (Pt),
 // stencil terms from the D array written by the stencil pass.
 template <typename SI, bool SYMM, typename DT>
@@ -141,7 +145,13 @@ struct DPt : Pt<SI, SYMM> {
   const DT* __restrict__ d;   // slot 0 of this point's block (add slot * dfs + p)
   long long dfs;              // slot stride
   template <typename T>
-  __device__ __forceinline__ T dv(int slot) const { return (T)__ldg(d + slot * dfs + this->p); }
+  __device__ __forceinline__ T dv(int slot) const {
+#if AMSS_D_STREAMING & 2
+    return (T)__ldcs(d + slot * dfs + this->p);
+#else
+    return (T)__ldg(d + slot * dfs + this->p);
+#endif
+  }
 };
 
 template <int D>
