@@ -134,7 +134,7 @@ constexpr int D_SLOTS_Z4C = D_SLOTS + 4;
 static_assert(doff(F_TZ) == D_SLOTS && doff(F_TZ + 1) == D_SLOTS_Z4C, "Z4c D slot layout");
 
 #ifndef AMSS_D_STREAMING   // the D array marked evict-first: bit 0 its stores, bit 1 its loads
-#define AMSS_D_STREAMING 0
+#define AMSS_D_STREAMING 3
 #endif
 
 // Accessor of the pointwise pass: centre values from the stage input (Pt),
