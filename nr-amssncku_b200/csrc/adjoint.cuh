@@ -196,15 +196,6 @@ __device__ __forceinline__ int ord_of(int f) { return (f & 1) ? 2 : ((f & 2) ? 1
 // the 2nd-order indicator is F2(q) - F4(q), F2 / F4 the "+-1 / +-2 fit in
 // every direction" products.
 
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 // In-plane arrays of a field kind: (slot offset within the field, or -1 / -2
 // for the shift's x / y component).  Roles: gx gy hxx hyy hxy hxz hyz adv bx by.
 template <int KIND>

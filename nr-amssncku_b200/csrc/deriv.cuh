@@ -8,7 +8,9 @@
 // negative indices hold the mirrored value times the field's parity, cells
 // past the block end are never read by the gated stencils and hold 0.  The
 // next plane is fetched into registers while the current one is computed,
-// so each plane costs one barrier.
+// so each plane costs one barrier.  The two-CTA form instead copies planes
+// straight into a 6-slot ring with cp.async, two planes ahead, where the
+// source needs no type conversion.
 //
 // z-direction work comes from registers: each thread keeps its column
 // f(k-3 .. k+3) and the windows of its x- and y-derivatives Dx f, Dy f at
@@ -44,12 +46,16 @@ constexpr int kDerivMinbLow = 2;
 #ifndef AMSS_DERIV_MINB_F32
 #define AMSS_DERIV_MINB_F32 3
 #endif
+#ifndef AMSS_DERIV_ASYNC   // 1: the plane ring is filled by cp.async where no type conversion is needed
+#define AMSS_DERIV_ASYNC 1
+#endif
 #ifndef AMSS_DERIV_PREFETCH   // planes beyond the register fetch whose tile rows are prefetched into L2 (0: none)
 #define AMSS_DERIV_PREFETCH 4
 #endif
 constexpr int DWMAX = 64;
 constexpr int DPLANE = 704;                 // >= (W + 6) (H + 6) for every admissible W
 constexpr int DRING = 5;                    // resident planes: k-1 (being replaced), k .. k+3
+constexpr int DRING_ASYNC = 6;              // cp.async ring: k .. k+3, k+4 landing, k+5 issued
 constexpr int DPER = (DPLANE + DTHREADS - 1) / DTHREADS;   // plane cells per thread
 
 // Tile shape of the stencil pass for a block of x extent ex0.
@@ -81,6 +87,22 @@ struct DerivItem {
 __host__ __device__ constexpr int dkind(int F) { return dslots(F) == 10 ? 0 : (dslots(F) == 4 ? 1 : 2); }
 
 __device__ __forceinline__ int ring_slot(int m) { return (m + 3) % DRING; }   // m >= -3
+
+// Asynchronous copies global -> shared of one 8- or 4-byte cell (zero-filled
+// when !valid; the source address is then not read).
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // A stencil term into D: written once here and read once by the pointwise
 // pass, so with AMSS_D_STREAMING bit 0 the store is marked evict-first
@@ -154,6 +176,70 @@ struct PlaneFetch {
   __device__ __forceinline__ void store(A* slot, int np) const { store_from(slot, np, v); }
 };
 
+// The same plane cells copied straight into the ring by cp.async when the
+// source type is the arithmetic type: no registers hold the plane in flight.
+// Cells past the block end are zero-filled by the copy; a mirrored cell is
+// negated after its copy lands, by the thread that issued it.
+template <typename A>
+struct PlaneAsync {
+  const A* src;
+  long long sz;
+  int ex2, np;
+  int off[DPER];     // i + j * ex0 of the (mirrored) cell, -1: none / past the end
+  unsigned neg;      // bit e: x/y mirroring flips the sign of cell e
+  bool zodd;         // field parity in z is odd
+
+  __device__ __forceinline__ void init(const A* s, int F, const int* ex, int x0, int y0, int sx, int n) {
+    src = s;
+    sz = (long long)ex[0] * ex[1];
+    ex2 = ex[2];
+    np = n;
+    zodd = soa_sign(F, 2) < 0;
+    neg = 0;
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      int o = -1;
+      if (t < n) {
+        int i = x0 - 3 + t % sx, j = y0 - 3 + t / sx;
+        bool m = false;
+        if (i < 0) { i = -i - 1; m ^= soa_sign(F, 0) < 0; }
+        if (j < 0) { j = -j - 1; m ^= soa_sign(F, 1) < 0; }
+        if (i < ex[0] && j < ex[1]) o = i + j * ex[0];
+        if (m) neg |= 1u << e;
+      }
+      off[e] = o;
+    }
+  }
+  // issue the copies of plane kk (negative: mirrored, past the end: 0) into slot
+  __device__ __forceinline__ void issue(int kk, A* slot) const {
+    const int k = kk < 0 ? -kk - 1 : kk;
+    const bool kin = k < ex2;
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      if (t < np) {
+        const bool ok = kin && off[e] >= 0;
+        const A* g = ok ? src + off[e] + k * sz : src;
+        if constexpr (sizeof(A) == 8) cp_async8(slot + t, g, ok);
+        else cp_async4(slot + t, g, ok);
+      }
+    }
+  }
+  // after the copies of plane kk landed: the signs of its mirrored cells
+  __device__ __forceinline__ void fix(int kk, A* slot) const {
+    const bool nz = kk < 0 && zodd;
+    if (!neg && !nz) return;
+    const int k = kk < 0 ? -kk - 1 : kk;
+    if (k >= ex2) return;
+#pragma unroll
+    for (int e = 0; e < DPER; ++e) {
+      const int t = threadIdx.x + e * DTHREADS;
+      if (t < np && off[e] >= 0 && (((neg >> e) & 1u) != 0) != nz) slot[t] = -slot[t];
+    }
+  }
+};
+
 // Upwinded term of one direction (lopsidediff.f90:321-481) over a line f(o),
 // o = -3 .. 3 relative to the point; f already includes the +1 of the
 // diagonal metric.  bd = beta * d12.
@@ -185,7 +271,7 @@ __device__ __forceinline__ A lop_term(const FN& f, A b, A bd, int idx, int lo, i
 // March one field of one tile.  A: stencil arithmetic type, S: type of the
 // field's source array, SI: type of the stage input (for the shift), T: type
 // of the D array.
-template <typename A, int KIND, typename T, typename S, typename SI>
+template <typename A, int KIND, bool ASYNC, typename T, typename S, typename SI>
 __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src, const SI* in, const double* bsh,
                                              int F, const DerivItem& it, T* D, long long dfs, A* ring) {
   const Coef<A>& C = pick<A>(B.C);
@@ -210,8 +296,16 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
   T* d = D + B.doff;
   const int own = (lj < H ? lj + 3 : 3) * DSX + (li + 3);   // idle threads read a valid cell
 
+  // ASYNC: cp.async fills the ring where the source needs no conversion (six
+  // slots: planes k .. k+3 read, k+4 landing, k+5 issued); otherwise the
+  // planes pass through registers (five slots)
+  constexpr bool kAsync = ASYNC && sizeof(A) == sizeof(S);
+  constexpr int R = kAsync ? DRING_ASYNC : DRING;
+  auto rs = [](int m) { return (m + 3) % R; };   // ring slot of plane m >= -3
   PlaneFetch<A, S> P;
-  P.init(src, F, B.b.ex, x0, y0, DSX, np);
+  PlaneAsync<A> PA;
+  if constexpr (kAsync) PA.init(reinterpret_cast<const A*>(src), F, B.b.ex, x0, y0, DSX, np);
+  else P.init(src, F, B.b.ex, x0, y0, DSX, np);
 
   A c[7];                  // column f(k-3 .. k+3)
   A fx4[5], fy4[5];        // 4th-order Dx f, Dy f at planes k-2 .. k+2 (KIND 0)
@@ -222,17 +316,42 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
   auto dx2 = [&](const A* q) { return C.d2[0] * (-q[-1] + q[1]); };
   auto dy2 = [&](const A* q) { return C.d2[1] * (-q[-DSX] + q[DSX]); };
 
-  // prologue: the loads of planes k0-3 .. k0+3 are issued together, then the
-  // planes enter the ring one at a time; the column gets k0-3 .. k0+3 and the
-  // derivative windows planes k0-2 .. k0+1
-  A pro[7][DPER];
+  // prologue: the column gets planes k0-3 .. k0+3 and the derivative windows
+  // planes k0-2 .. k0+1.  Register form: the loads of the seven planes are
+  // issued together, then the planes enter the ring one at a time.  cp.async
+  // form: planes k0-3 .. k0+2 fill the six slots at once; once they are read,
+  // k0+3 and k0+4 take the slots of k0-3 and k0-2.
+  A pro[kAsync ? 1 : 7][DPER];
+  if constexpr (kAsync) {
 #pragma unroll
-  for (int m = -3; m <= 3; ++m) P.fetch_to(k0 + m, pro[m + 3]);
+    for (int m = -3; m <= 2; ++m) PA.issue(k0 + m, ring + rs(k0 + m) * DPLANE);
+    cp_async_commit();
+    cp_async_wait<0>();
+#pragma unroll
+    for (int m = -3; m <= 2; ++m) PA.fix(k0 + m, ring + rs(k0 + m) * DPLANE);
+    __syncthreads();
+  } else {
+#pragma unroll
+    for (int m = -3; m <= 3; ++m) P.fetch_to(k0 + m, pro[m + 3]);
+  }
 #pragma unroll
   for (int m = -3; m <= 3; ++m) {
-    A* slot = ring + ring_slot(k0 + m) * DPLANE;
-    P.store_from(slot, np, pro[m + 3]);
-    __syncthreads();
+    A* slot = ring + rs(k0 + m) * DPLANE;
+    if constexpr (kAsync) {
+      if (m == 3) {
+        __syncthreads();   // planes k0-3, k0-2 are read: their slots take k0+3, k0+4
+        PA.issue(k0 + 3, slot);
+        cp_async_commit();
+        PA.issue(k0 + 4, ring + rs(k0 + 4) * DPLANE);
+        cp_async_commit();
+        cp_async_wait<1>();
+        PA.fix(k0 + 3, slot);
+        __syncthreads();
+      }
+    } else {
+      P.store_from(slot, np, pro[m + 3]);
+      __syncthreads();
+    }
     const A* q = slot + own;
     const A cm = q[0];
 #pragma unroll
@@ -253,7 +372,13 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
 
 #pragma unroll 1
   for (int k = k0; k < kend; ++k) {
-    P.fetch(k + 4);   // in flight while plane k is computed
+    // in flight while plane k is computed: plane k+4 (registers) or k+5 (cp.async)
+    if constexpr (kAsync) {
+      PA.issue(k + 5, ring + rs(k + 5) * DPLANE);
+      cp_async_commit();
+    } else {
+      P.fetch(k + 4);
+    }
 #if AMSS_DERIV_PREFETCH
     {
       // warp 0 asks L2 for the tile rows (with halo) of plane k+4+AMSS_DERIV_PREFETCH,
@@ -273,11 +398,11 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
       }
     }
 #endif
-    const A* qk = ring + ring_slot(k) * DPLANE + own;
-    c[6] = ring[ring_slot(k + 3) * DPLANE + own];
+    const A* qk = ring + rs(k) * DPLANE + own;
+    c[6] = ring[rs(k + 3) * DPLANE + own];
     if constexpr (KIND == 0) {
-      const A* q2 = ring + ring_slot(k + 2) * DPLANE + own;
-      const A* q1 = ring + ring_slot(k + 1) * DPLANE + own;
+      const A* q2 = ring + rs(k + 2) * DPLANE + own;
+      const A* q1 = ring + rs(k + 1) * DPLANE + own;
       fx4[4] = dx4(q2); fy4[4] = dy4(q2); fx2[2] = dx2(q1); fy2[2] = dy2(q1);
     }
     const bool on_face = face_xy || ((fm & 4) && k == ex2 - 1) || ((fm & 32) && k == 0);
@@ -369,10 +494,19 @@ __device__ __forceinline__ void deriv_column(const StepBlock<T>& B, const S* src
 #pragma unroll
       for (int t = 0; t < 2; ++t) { fx2[t] = fx2[t + 1]; fy2[t] = fy2[t + 1]; }
     }
-    // plane k+4 replaces plane k-1, which no thread reads in this iteration
-    P.store(ring + ring_slot(k + 4) * DPLANE, np);
+    // plane k+4 is complete for the next iteration: it replaced plane k-1
+    // (register form) or landed (cp.async form), and no thread reads that slot
+    // in this iteration
+    if constexpr (kAsync) {
+      cp_async_wait<1>();
+      PA.fix(k + 4, ring + rs(k + 4) * DPLANE);
+    } else {
+      P.store(ring + ring_slot(k + 4) * DPLANE, np);
+    }
     __syncthreads();
   }
+  // the copies still in flight land before the ring is reused
+  if constexpr (kAsync) cp_async_wait<0>();
 }
 
 // Stencil pass over a work list of (block, tile, field) items, ordered by
@@ -382,6 +516,9 @@ __global__ void __launch_bounds__(DTHREADS, MINB) k_deriv(const StepBlock<T>* __
                                                       const DerivItem* __restrict__ items, int nitems, int sub,
                                                       T* __restrict__ D, long long dfs) {
   extern __shared__ __align__(16) unsigned char smem[];
+  // the two-CTA form fills its ring by cp.async; the forms with more CTAs keep
+  // the register path, whose smaller ring leaves L1 to their spills
+  constexpr bool kAsyncForm = AMSS_DERIV_ASYNC && MINB == kDerivMinbLow;
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const DerivItem it = items[w];
     const StepBlock<T>& B = blocks[it.block];
@@ -396,22 +533,24 @@ __global__ void __launch_bounds__(DTHREADS, MINB) k_deriv(const StepBlock<T>* __
         // wide fields of the mixed form: FP64 source (state, or the FP64 side stage) and arithmetic
         const double* src = sizeof(SI) == 4 ? B.side[sub == 2 ? 1 : 0] + side_slot(F) * fs
                                             : (const double*)in + F * fs;
-        deriv_column<double, 0>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<double*>(smem));
+        deriv_column<double, 0, kAsyncForm>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<double*>(smem));
         __syncthreads();
         continue;
       }
     }
     const SI* src = in + F * fs;
     switch (dkind(F)) {
-      case 0: deriv_column<T, 0>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
-      case 1: deriv_column<T, 1>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
-      default: deriv_column<T, 2>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 0: deriv_column<T, 0, kAsyncForm>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
+      case 1: deriv_column<T, 1, kAsyncForm>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
+      default: deriv_column<T, 2, kAsyncForm>(B, src, in, bsh, F, it, D, dfs, reinterpret_cast<T*>(smem)); break;
     }
     __syncthreads();
   }
 }
 
-// Shared memory of k_deriv: the plane ring in the widest arithmetic type.
+// Shared memory of k_deriv: the plane ring in the widest arithmetic type, for
+// the two-CTA form (cp.async ring) and the others (register path).
+constexpr size_t kDerivSmemLow = (size_t)(AMSS_DERIV_ASYNC ? DRING_ASYNC : DRING) * DPLANE * sizeof(double);
 constexpr size_t kDerivSmem = (size_t)DRING * DPLANE * sizeof(double);
 
 }  // namespace amss

@@ -200,7 +200,8 @@ template <typename T, typename SS>
 cudaError_t launch_deriv(const void* blocks, const DerivItem* items, int nitems, int sub, void* D, long long dfs,
                          int grid, cudaStream_t s, int occ) {
   const StepBlock<T>* bl = (const StepBlock<T>*)blocks;
-  const size_t smem = kDerivSmem;   // < 48 KB: no opt-in attribute needed
+  // both < 48 KB: no opt-in attribute needed
+  const size_t smem = occ ? kDerivSmem : kDerivSmemLow;
   constexpr int hi = sizeof(T) == 8 ? AMSS_DERIV_MINB_F64 : AMSS_DERIV_MINB_F32;
   if (sub == 0) {
     if (occ) k_deriv<T, double, hi><<<grid, DTHREADS, smem, s>>>(bl, items, nitems, sub, (T*)D, dfs);
