@@ -303,10 +303,13 @@ int amss_engine_get_level_occupancy(amss_engine* e, int level, int* occ);
  * cells of the owning block's physical box and every buffer cell prolonged,
  * the final substep updates only each owned block's cells within that
  * distance; the other cells' new values would be overwritten unread, so the
- * coarse step's results are the same bit for bit.  *pad = -1: whole arrays
- * (level 0, or a hierarchy that fails the test).  A single level step
- * (amss_engine_step_level) always updates whole arrays.  *points: the cells
- * the final substep updates on this rank's blocks of the level. */
+ * coarse step's results are the same bit for bit.  *pad = -1: no such
+ * regions (level 0, or a hierarchy that fails the test).  A single level step
+ * (amss_engine_step_level) never uses them.  Every substep (the final one
+ * too, where it has no regions) skips a block's ghost cells when commit finds
+ * that the same-level sync after it overwrites every ghost cell of the level.
+ * *points: the cells a coarse step's final substep updates on this rank's
+ * blocks of the level. */
 int amss_engine_level_final_region(amss_engine* e, int level, int* pad, long long* points);
 
 /* Moving-box regrid (cgh::Regrid_Onelevel, cgh.C:1304-1506, whose data step is

@@ -194,7 +194,8 @@ class Engine:
     def final_region(self, level):
         """(pad, points) of a level's final substep in a coarse step: pad 2,
         the owned cells within 2 of the physical box (the rest are overwritten
-        by the prolongation unread); -1, whole arrays.  points: the cells it
+        by the prolongation unread); -1, no such regions (the owned cells, where
+        the sync fills every ghost, else whole arrays).  points: the cells it
         updates on this engine's blocks."""
         pad, pts = ctypes.c_int(), ctypes.c_longlong()
         check(lib().amss_engine_level_final_region(self._h, level, ctypes.byref(pad), ctypes.byref(pts)),

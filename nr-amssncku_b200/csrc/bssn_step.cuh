@@ -178,12 +178,17 @@ struct StepBlock {
   int lev0;           // 1: Sommerfeld rule on the patch faces; 0: freeze them at u0
   int nf;             // evolved fields: 24 (BSSN) or 25 (Z4c, Theta last)
   int dw;             // stencil-pass tile width (deriv_tile_w of ex[0])
-  int rlo[3], rn[3];  // region of the final substep's region tiles (array indices [rlo, rlo + rn))
+  // regions of region tiles, array indices [rlo, rlo + rn): [0] the final
+  // substep's, [1] the block's owned cells (its ghosts are synchronised)
+  int rlo[2][3], rn[2][3];
 };
 
 // Tile of a pointwise list: tile.x = table index, tile.y = first point.
-// With kRegionTile set in tile.x, the points count the block's final-substep
-// region [rlo, rlo + rn) in x-fastest order instead of its whole array.
+// With kRegionTile set in tile.x, the points count one of the block's regions
+// in x-fastest order instead of its whole array: the final substep's, or with
+// kOwnRegion also set its owned cells.
 constexpr int kRegionTile = 1 << 30;
+constexpr int kOwnRegion = 1 << 29;
+constexpr int kTileIndex = kOwnRegion - 1;
 
 }  // namespace amss

@@ -130,6 +130,8 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.ditems) cudaFree(L.ditems);
     if (L.dtiles_f) cudaFree(L.dtiles_f);
     if (L.ditems_f) cudaFree(L.ditems_f);
+    if (L.dtiles_s) cudaFree(L.dtiles_s);
+    if (L.ditems_s) cudaFree(L.ditems_s);
     if (L.dfaces) cudaFree(L.dfaces);
     if (L.dregion) cudaFree(L.dregion);
     if (L.dregion_first) cudaFree(L.dregion_first);
@@ -265,17 +267,25 @@ static int level_tile_w(const ELevel& L, int ex0) {
 // z extent is cut into L.zsplit slabs of near-equal height (each slab marches
 // its own planes after a 7-plane prologue): more, shorter work items for
 // levels whose items would otherwise fill the last wave of CTAs poorly.
-// Stencil-pass work items over each owned block's array, or (fin) over its
-// final-substep region: x-y tiles of the level's tile width, z-slabs, ordered by
-// field.
-static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L, bool fin = false) {
+// The cells of a block a list covers: 0 its array, 1 its owned cells, 2 its
+// final-substep region (global level indices).
+static Box list_box(const amss_engine* e, const ELevel& L, const EBlock& b, int mode) {
+  if (mode == 1) return intersect(b.own, b.array());
+  if (mode == 2) return final_region(e, L, b);
+  return b.array();
+}
+
+// Stencil-pass work items over each of this rank's blocks of a level: over its
+// array (mode 0), its owned cells (1) or its final-substep region (2); x-y tiles
+// of the level's tile width, z-slabs, ordered by field.
+static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L, int mode = 0) {
   static const int order[25] = {F_CHI, F_LAP, F_BETAX, F_BETAY, F_BETAZ, F_GXX, F_GXY, F_GXZ,
                                 F_GYY, F_GYZ, F_GZZ, F_TRK, F_GAMX, F_GAMY, F_GAMZ, F_TZ, F_AXX,
                                 F_AXY, F_AXZ, F_AYY, F_AYZ, F_AZZ, F_DTSFX, F_DTSFY, F_DTSFZ};
   std::vector<DerivItem> tiles;
   for (size_t m = 0; m < L.own.size(); ++m) {
     const EBlock& b = e->blocks[L.own[m]];
-    if (!fin) {
+    if (mode == 0) {
       const int tw = level_tile_w(L, b.ex[0]), th = DTHREADS / tw;
       const int ns = std::max(1, std::min(L.zsplit, b.ex[2] / kMinSlab));
       for (int z = 0; z < ns; ++z) {
@@ -286,7 +296,7 @@ static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L, bool 
       }
       continue;
     }
-    const Box r = final_region(e, L, b);
+    const Box r = list_box(e, L, b, mode);
     if (r.empty()) continue;
     int lo[3], n[3];
     for (int d = 0; d < 3; ++d) { lo[d] = r.lo[d] - b.org[d]; n[d] = r.hi[d] - r.lo[d]; }
@@ -314,7 +324,7 @@ static std::vector<DerivItem> deriv_items(amss_engine* e, const ELevel& L, bool 
 template <typename T>
 static int build_table(amss_engine* e, ELevel& L, int level) {
   std::vector<StepBlock<T>> tab;
-  std::vector<int2> tiles, tiles_f;
+  std::vector<int2> tiles, tiles_f, tiles_s;
   std::vector<int2> faces;
   std::vector<DerivItem> items;
   long long doff = 0;
@@ -344,10 +354,12 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     s.lev0 = level == 0 ? 1 : 0;
     s.nf = e->nf;
     s.dw = level_tile_w(L, b.ex[0]);
-    const Box fr = final_region(e, L, b);
-    for (int d = 0; d < 3; ++d) {
-      s.rlo[d] = fr.lo[d] - b.org[d];
-      s.rn[d] = fr.empty() ? 0 : fr.hi[d] - fr.lo[d];
+    for (int g = 0; g < 2; ++g) {
+      const Box r = list_box(e, L, b, g == 0 ? 2 : 1);
+      for (int d = 0; d < 3; ++d) {
+        s.rlo[g][d] = r.lo[d] - b.org[d];
+        s.rn[g][d] = r.empty() ? 0 : r.hi[d] - r.lo[d];
+      }
     }
     if (b.lowsym) L.symm = true;
     tab.push_back(s);
@@ -355,8 +367,12 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     const long long tstep = e->prm.kernel == 0 ? kPointwiseTile : 128;
     for (long long p = 0; p < b.npts; p += tstep) tiles.push_back(make_int2((int)m, (int)p));
     if (L.final_pad >= 0) {
-      const long long nr = (long long)s.rn[0] * s.rn[1] * s.rn[2];
+      const long long nr = (long long)s.rn[0][0] * s.rn[0][1] * s.rn[0][2];
       for (long long q = 0; q < nr; q += tstep) tiles_f.push_back(make_int2((int)m | kRegionTile, (int)q));
+    }
+    if (L.own_ok) {
+      const long long nr = (long long)s.rn[1][0] * s.rn[1][1] * s.rn[1][2];
+      for (long long q = 0; q < nr; q += tstep) tiles_s.push_back(make_int2((int)m | kRegionTile | kOwnRegion, (int)q));
     }
     if (b.face_mask) {
       const int fm = b.face_mask;
@@ -371,10 +387,13 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
     }
   }
   items = deriv_items(e, L);
-  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, true) : std::vector<DerivItem>();
+  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, 2) : std::vector<DerivItem>();
+  const std::vector<DerivItem> items_s = L.own_ok ? deriv_items(e, L, 1) : std::vector<DerivItem>();
   L.ntiles = (int)tiles.size();
   L.ntiles_f = (int)tiles_f.size();
   L.nditems_f = (int)items_f.size();
+  L.ntiles_s = (int)tiles_s.size();
+  L.nditems_s = (int)items_s.size();
   {
     // constraint-norm region of each table block, in array indices.  A block
     // added by bbox: 3 ghost cells off each side, unless the side's outer cell
@@ -441,6 +460,14 @@ static int build_table(amss_engine* e, ELevel& L, int level) {
   if (!items_f.empty()) {
     AMSS_CK(cudaMalloc(&L.ditems_f, items_f.size() * sizeof(DerivItem)));
     AMSS_CK(cudaMemcpy(L.ditems_f, items_f.data(), items_f.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  }
+  if (!tiles_s.empty()) {
+    AMSS_CK(cudaMalloc(&L.dtiles_s, tiles_s.size() * sizeof(int2)));
+    AMSS_CK(cudaMemcpy(L.dtiles_s, tiles_s.data(), tiles_s.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
+  if (!items_s.empty()) {
+    AMSS_CK(cudaMalloc(&L.ditems_s, items_s.size() * sizeof(DerivItem)));
+    AMSS_CK(cudaMemcpy(L.ditems_s, items_s.data(), items_s.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   }
   return 0;
 }
@@ -743,12 +770,14 @@ static int step_level_impl(amss_engine* e, int level, double dt, bool fin = fals
   const bool split = e->prm.kernel == 0;
   const bool track = e->ntrack > 0 && level == e->track_level;
   for (int sub = 0; sub < 4; ++sub) {
-    // the final substep over the regions, where the level has them
+    // the final substep over the regions, where the level has them; the
+    // others over the owned cells, where the sync after them fills the ghosts
     const bool reg = fin && sub == 3 && L.final_pad >= 0;
-    const DerivItem* ditems = reg ? L.ditems_f : L.ditems;
-    const int nditems = reg ? L.nditems_f : L.nditems;
-    const int2* tiles = reg ? L.dtiles_f : L.dtiles;
-    const int ntiles = reg ? L.ntiles_f : L.ntiles;
+    const bool own = !reg && L.own_ok;
+    const DerivItem* ditems = reg ? L.ditems_f : own ? L.ditems_s : L.ditems;
+    const int nditems = reg ? L.nditems_f : own ? L.nditems_s : L.nditems;
+    const int2* tiles = reg ? L.dtiles_f : own ? L.dtiles_s : L.dtiles;
+    const int ntiles = reg ? L.ntiles_f : own ? L.ntiles_s : L.ntiles;
     const int dgrid = std::min(nditems, e->sm_count * 16);
     const int grid = std::min(ntiles, e->sm_count * 8);
     if (!work) {
@@ -874,18 +903,25 @@ extern "C" int amss_engine_set_level_tiling(amss_engine* e, int level, int tile_
   L.tile_w = tile_w;
   L.zsplit = zsplit;
   const std::vector<DerivItem> items = deriv_items(e, L);
-  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, true) : std::vector<DerivItem>();
+  const std::vector<DerivItem> items_f = L.final_pad >= 0 ? deriv_items(e, L, 2) : std::vector<DerivItem>();
+  const std::vector<DerivItem> items_s = L.own_ok ? deriv_items(e, L, 1) : std::vector<DerivItem>();
   if (L.ditems) cudaFree(L.ditems);
   if (L.ditems_f) cudaFree(L.ditems_f);
-  L.ditems = L.ditems_f = nullptr;
+  if (L.ditems_s) cudaFree(L.ditems_s);
+  L.ditems = L.ditems_f = L.ditems_s = nullptr;
   L.nditems = (int)items.size();
   L.nditems_f = (int)items_f.size();
+  L.nditems_s = (int)items_s.size();
   if (items.empty()) return 0;
   AMSS_CK(cudaMalloc(&L.ditems, items.size() * sizeof(DerivItem)));
   AMSS_CK(cudaMemcpy(L.ditems, items.data(), items.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   if (!items_f.empty()) {
     AMSS_CK(cudaMalloc(&L.ditems_f, items_f.size() * sizeof(DerivItem)));
     AMSS_CK(cudaMemcpy(L.ditems_f, items_f.data(), items_f.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
+  }
+  if (!items_s.empty()) {
+    AMSS_CK(cudaMalloc(&L.ditems_s, items_s.size() * sizeof(DerivItem)));
+    AMSS_CK(cudaMemcpy(L.ditems_s, items_s.data(), items_s.size() * sizeof(DerivItem), cudaMemcpyHostToDevice));
   }
   return e->prm.precision == 1 ? patch_table_dw<float>(e, L) : patch_table_dw<double>(e, L);
 }
@@ -898,8 +934,9 @@ extern "C" int amss_engine_level_final_region(amss_engine* e, int level, int* pa
   if (pad) *pad = L.final_pad;
   if (points) {
     long long n = 0;
+    const int mode = L.final_pad >= 0 ? 2 : L.own_ok ? 1 : 0;
     for (int b : L.own) {
-      const Box r = final_region(e, L, e->blocks[b]);
+      const Box r = list_box(e, L, e->blocks[b], mode);
       if (!r.empty()) n += (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
     }
     *points = n;

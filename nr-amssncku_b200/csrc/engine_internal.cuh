@@ -129,6 +129,13 @@ struct ELevel {
   int ntiles_f = 0;
   DerivItem* ditems_f = nullptr;   // and its stencil-pass items
   int nditems_f = 0;
+  // The substeps over each block's owned cells only: the same-level sync
+  // after every substep overwrites all of its ghost cells (plan_final_regions).
+  bool own_ok = false;
+  int2* dtiles_s = nullptr;     // owned-cell tiles of the pointwise pass
+  int ntiles_s = 0;
+  DerivItem* ditems_s = nullptr;   // and the stencil-pass items
+  int nditems_s = 0;
   int tile_w = 0;               // stencil-pass tile width (0: deriv_tile_w of each block's x extent)
   int zsplit = 1;               // z-slabs per block in the stencil pass
   int docc = 0;                 // stencil-pass occupancy form: 0 two resident CTAs, 1 more (deriv.cuh)
@@ -197,7 +204,8 @@ int run_xfer(amss_engine* e, int op, int arg);        // arg: sync buffer, restr
 void release_xfers(amss_engine* e);
 void amss_xfer_detach(amss_engine* e);              // leaves its group, destroys its NCCL communicator
 int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int nf = 0, bool runs = false);
-// Sets each level's final_pad where the final-substep regions are safe.
+// Sets each level's final_pad where the final-substep regions are safe, and
+// own_ok where the same-level sync covers every ghost cell.
 void plan_final_regions(amss_engine* e);
 // The final-substep region of a block (global level indices; empty: none).
 Box final_region(const amss_engine* e, const ELevel& L, const EBlock& b);

@@ -16,22 +16,29 @@
 
 namespace amss {
 
-// Points of a tile list's range in a block: its array, or its region.
+// Region of a tile: -1 the whole array, else the index into StepBlock::rlo/rn.
+__device__ __forceinline__ int tile_region(int x) {
+  return (x & kRegionTile) ? ((x & kOwnRegion) ? 1 : 0) : -1;
+}
+
+// Points of a tile list's range in a block: its array, or one of its regions.
 template <typename T>
-__device__ __forceinline__ long long tile_count(const StepBlock<T>& B, bool region) {
-  return region ? (long long)B.rn[0] * B.rn[1] * B.rn[2] : B.npts;
+__device__ __forceinline__ long long tile_count(const StepBlock<T>& B, int rg) {
+  return rg >= 0 ? (long long)B.rn[rg][0] * B.rn[rg][1] * B.rn[rg][2] : B.npts;
 }
 
 // Array point of entry q of a tile's point range, or -1 past its end.
 template <typename T>
-__device__ __forceinline__ long long tile_point(const StepBlock<T>& B, bool region, long long q) {
-  if (q >= tile_count(B, region)) return -1;
-  if (!region) return q;
-  const long long n01 = (long long)B.rn[0] * B.rn[1];
+__device__ __forceinline__ long long tile_point(const StepBlock<T>& B, int rg, long long q) {
+  if (q >= tile_count(B, rg)) return -1;
+  if (rg < 0) return q;
+  const int* lo = B.rlo[rg];
+  const int* n = B.rn[rg];
+  const long long n01 = (long long)n[0] * n[1];
   const int k = (int)(q / n01);
   const long long r = q - (long long)k * n01;
-  const int j = (int)(r / B.rn[0]), i = (int)(r - (long long)j * B.rn[0]);
-  return (long long)(i + B.rlo[0]) + (long long)B.b.ex[0] * ((long long)(j + B.rlo[1]) + (long long)B.b.ex[1] * (k + B.rlo[2]));
+  const int j = (int)(r / n[0]), i = (int)(r - (long long)j * n[0]);
+  return (long long)(i + lo[0]) + (long long)B.b.ex[0] * ((long long)(j + lo[1]) + (long long)B.b.ex[1] * (k + lo[2]));
 }
 
 // Fused RK4 substep over a tile list of one level.  Substep `sub` reads
@@ -46,8 +53,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
                                                                     long long dfs) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
-    const bool region = (tile.x & kRegionTile) != 0;
-    const StepBlock<T>& B = blocks[tile.x & ~kRegionTile];
+    const int region = tile_region(tile.x);
+    const StepBlock<T>& B = blocks[tile.x & kTileIndex];
 #if AMSS_POINTWISE_PREFETCH
     // split form: pull the rows of a tile (D slots, stage input, u0, K) into
     // L2 -- the next tile's while this one computes, or this tile's before its
@@ -61,8 +68,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? AMSS_SUBSTEP_MINB_F32 : 
       const int tn = pass == 0 ? t : t + (int)gridDim.x;
       if (threadIdx.x < 32 && tn < ntiles) {
         const int2 nt = tiles[tn];
-        const bool nreg = (nt.x & kRegionTile) != 0;
-        const StepBlock<T>& N = blocks[nt.x & ~kRegionTile];
+        const int nreg = tile_region(nt.x);
+        const StepBlock<T>& N = blocks[nt.x & kTileIndex];
         const long long fs = N.b.fs;
         const int cur = N.lvl[0];
         const SI* nin = sub == 0 ? (const SI*)N.tl[cur] : (const SI*)N.stage[sub == 2 ? 1 : 0];

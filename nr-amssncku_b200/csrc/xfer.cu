@@ -229,7 +229,26 @@ Box final_region(const amss_engine* e, const ELevel& L, const EBlock& b) {
 }
 
 void plan_final_regions(amss_engine* e) {
-  for (auto& kv : e->levels) kv.second.final_pad = -1;
+  for (auto& kv : e->levels) {
+    kv.second.final_pad = -1;
+    kv.second.own_ok = false;
+  }
+  // owned cells only: owned boxes disjoint and inside the arrays, and the
+  // sync's boxes into each block cover every cell of its array it does not own
+  for (auto& kv : e->levels) {
+    ELevel& L = kv.second;
+    bool ok = !L.blocks.empty();
+    std::map<int, long long> cover;
+    for (const AmrBox& b : sync_boxes(e, L)) cover[b.dst] += (long long)b.n[0] * b.n[1] * b.n[2];
+    for (size_t a = 0; a < L.blocks.size() && ok; ++a) {
+      const EBlock& A = e->blocks[L.blocks[a]];
+      if (volume(intersect(A.own, A.array())) != volume(A.own) || volume(A.own) == 0) ok = false;
+      if (cover[L.blocks[a]] != volume(A.array()) - volume(A.own)) ok = false;
+      for (size_t b = a + 1; b < L.blocks.size() && ok; ++b)
+        if (volume(intersect(A.own, e->blocks[L.blocks[b]].own)) != 0) ok = false;
+    }
+    L.own_ok = ok;
+  }
   for (auto& kv : e->levels) {
     const int l = kv.first;
     ELevel& L = kv.second;

@@ -10,7 +10,8 @@ the finer level's prolongation, prolong3: coarse k-3 .. k+3) and that the
 prolongation into the level covers its buffer cells.  Checked here: the amr
 bench hierarchy gets regions on every refined level with the expected cell
 counts; the counts divide among ranks; a level whose child's buffer reaches
-its physical boundary keeps whole arrays."""
+its physical boundary keeps no regions (its owned cells, whose ghosts the
+sync fills)."""
 import numpy as np
 
 from amss_b200 import dist as D
@@ -28,6 +29,11 @@ def expected_points(H, lv, pad, blocks=None):
             hi = [min(b.own_hi[d], p.hi[d] + pad, b.org[d] + b.ex[d]) for d in range(3)]
             n += int(np.prod([max(0, hi[d] - lo[d]) for d in range(3)]))
     return n
+
+
+def owned_points(H, lv):
+    return sum(int(np.prod([H.blocks[bi].own_hi[d] - H.blocks[bi].own_lo[d] for d in range(3)]))
+               for p in H.levels[lv] for bi in p.blocks)
 
 
 def amr_hierarchy():
@@ -49,7 +55,10 @@ def test_amr_levels_take_final_regions():
     H = amr_hierarchy()
     P = D.Plan.of(H, 0, 1, [0] * len(H.blocks))
     try:
-        assert P.final_region(0) == (-1, H.points(0))
+        # level 0 has no regions; its ghost cells are synchronised, so the final
+        # substep updates the owned cells
+        assert owned_points(H, 0) < H.points(0)
+        assert P.final_region(0) == (-1, owned_points(H, 0))
         for lv in range(1, len(H.levels)):
             pad, pts = P.final_region(lv)
             assert pad == 2
@@ -75,11 +84,11 @@ def test_rank_plans_count_their_own_blocks():
     assert all(tot[lv] == expected_points(H, lv, 2) for lv in range(1, len(H.levels)))
 
 
-def test_level_read_past_its_pad_keeps_whole_arrays():
+def test_level_read_past_its_pad_keeps_no_regions():
     H = touching_hierarchy()
     P = D.Plan.of(H, 0, 1, [0] * len(H.blocks))
     try:
-        assert P.final_region(1) == (-1, H.points(1))
+        assert P.final_region(1) == (-1, owned_points(H, 1))
         assert P.final_region(2) == (2, expected_points(H, 2, 2))
     finally:
         P.close()

@@ -381,7 +381,10 @@ def test_final_substep_regions_in_use():
     H = small_hierarchy()
     e = amss_b200.Engine.from_hierarchy(H, eps=0.1)
     try:
-        assert e.final_region(0) == (-1, H.points(0))
+        # level 0: no regions; its ghosts are synchronised, so its owned cells
+        own0 = sum(int(np.prod([H.blocks[bi].own_hi[d] - H.blocks[bi].own_lo[d] for d in range(3)]))
+                   for p in H.levels[0] for bi in p.blocks)
+        assert e.final_region(0) == (-1, own0)
         for lv in (1, 2):
             pad, pts = e.final_region(lv)
             assert pad == 2 and 0 < pts < H.points(lv)
@@ -412,7 +415,7 @@ def test_single_level_step_updates_every_cell(fp64_reference):
 
 def test_level_without_regions_matches_oracle():
     """Level 2's buffered box reaches level 1's physical boundary: level 1
-    keeps whole arrays in its final substep, level 2 takes regions; two
+    takes no regions in its final substep, level 2 does; two
     coarse steps against the oracle."""
     from amss_b200.hierarchy import Hierarchy
     H = Hierarchy(-8.0, 0.5)
