@@ -92,3 +92,18 @@ def test_level_read_past_its_pad_keeps_no_regions():
         assert P.final_region(2) == (2, expected_points(H, 2, 2))
     finally:
         P.close()
+
+
+def test_blocks_added_by_bbox_keep_whole_arrays():
+    """Blocks added by bounding box (each its own patch, cells numbered from
+    0) have no same-level sync to rely on: their substeps cover whole arrays."""
+    P = D.Plan(eps=0.1)
+    try:
+        a = [-2.0, -2.0, -2.0, 1.0, 1.0, 1.0]
+        b = [0.0, -2.0, -2.0, 3.0, 1.0, 1.0]
+        P.add_block(0, (12, 12, 12), a, a)
+        P.add_block(0, (12, 12, 12), b, b)
+        P.commit()
+        assert P.final_region(0) == (-1, 2 * 12 ** 3)
+    finally:
+        P.close()
