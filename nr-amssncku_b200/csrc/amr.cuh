@@ -196,7 +196,27 @@ __global__ void k_amr_restrict(const AmrBlock* __restrict__ blocks, const AmrBox
 // Parent state at the child's intermediate time into K (prepare_inter_time_level,
 // Parallel.C:4329-4441): average2 (fmisc.f90:1569-1592, 3/8 new + 3/4 old
 // - 1/8 older) once the level has two steps behind it, else average
-// (fmisc.f90:1532, (new + old)/2).  One thread per block point.
+// (fmisc.f90:1532, (new + old)/2), at array point p of block B.
+__device__ __forceinline__ void timeinterp_point(const AmrBlock& B, long long p) {
+  const int cur = B.lvl[0];
+  const double* f1 = B.tl[cur];
+  const double* f2 = B.tl[(cur + 2) % 3];
+  const double* f3 = B.tl[(cur + 1) % 3];
+  if (B.lvl[1] >= 2) {
+    const double C1 = 3.0 / 8.0, C2 = 3.0 / 4.0, C3 = -1.0 / 8.0;
+    for (int f = 0; f < B.nf; ++f) {
+      const long long o = f * B.fs + p;
+      B.K[o] = __dadd_rn(__dadd_rn(__dmul_rn(C1, f1[o]), __dmul_rn(C2, f2[o])), __dmul_rn(C3, f3[o]));
+    }
+  } else {
+    for (int f = 0; f < B.nf; ++f) {
+      const long long o = f * B.fs + p;
+      B.K[o] = __dmul_rn(0.5, __dadd_rn(f1[o], f2[o]));
+    }
+  }
+}
+
+// Over every point of a level's blocks: one thread per block point.
 __global__ void k_amr_timeinterp(const AmrBlock* __restrict__ blocks, const int2* __restrict__ tiles, int ntiles) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int2 tile = tiles[t];
@@ -204,22 +224,26 @@ __global__ void k_amr_timeinterp(const AmrBlock* __restrict__ blocks, const int2
     const long long p = (long long)tile.y + threadIdx.x;
     const long long np = (long long)B.ex[0] * B.ex[1] * B.ex[2];
     if (p >= np) continue;
-    const int cur = B.lvl[0];
-    const double* f1 = B.tl[cur];
-    const double* f2 = B.tl[(cur + 2) % 3];
-    const double* f3 = B.tl[(cur + 1) % 3];
-    if (B.lvl[1] >= 2) {
-      const double C1 = 3.0 / 8.0, C2 = 3.0 / 4.0, C3 = -1.0 / 8.0;
-      for (int f = 0; f < B.nf; ++f) {
-        const long long o = f * B.fs + p;
-        B.K[o] = __dadd_rn(__dadd_rn(__dmul_rn(C1, f1[o]), __dmul_rn(C2, f2[o])), __dmul_rn(C3, f3[o]));
-      }
-    } else {
-      for (int f = 0; f < B.nf; ++f) {
-        const long long o = f * B.fs + p;
-        B.K[o] = __dmul_rn(0.5, __dadd_rn(f1[o], f2[o]));
-      }
+    timeinterp_point(B, p);
+  }
+}
+
+// Over boxes of cells (dst = the block; the cells a finer level's
+// prolongation reads from it): one thread per box cell.
+__global__ void k_amr_timeinterp_boxes(const AmrBlock* __restrict__ blocks, const AmrBox* __restrict__ boxes,
+                                       const int2* __restrict__ tiles, int ntiles, unsigned* status) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int2 tile = tiles[t];
+    const AmrBox& bx = boxes[tile.x];
+    const int q = tile.y + threadIdx.x;
+    if (q >= bx.n[0] * bx.n[1] * bx.n[2]) continue;
+    const AmrBlock& B = blocks[bx.dst];
+    const int x = bx.lo[0] + q % bx.n[0], y = bx.lo[1] + (q / bx.n[0]) % bx.n[1], z = bx.lo[2] + q / (bx.n[0] * bx.n[1]);
+    if (!amr_inside(B, x, y, z)) {
+      atomicOr(status, ST_BAD_ARG);
+      continue;
     }
+    timeinterp_point(B, amr_idx(B, x, y, z));
   }
 }
 

@@ -36,6 +36,13 @@ cudaError_t launch_amr_timeinterp(const AmrBlock* blocks, const int2* tiles, int
   return cudaGetLastError();
 }
 
+cudaError_t launch_amr_timeinterp_boxes(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
+                                        unsigned* status, cudaStream_t s) {
+  if (ntiles == 0) return cudaSuccess;
+  k_amr_timeinterp_boxes<<<amr_grid(ntiles), 128, 0, s>>>(blocks, boxes, tiles, ntiles, status);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_amr_enforce(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s) {
   if (ntiles == 0) return cudaSuccess;
   k_amr_enforce<<<amr_grid(ntiles), 128, 0, s>>>(blocks, tiles, ntiles);

@@ -51,6 +51,8 @@ cudaError_t launch_amr_prolong(const AmrBlock* blocks, const AmrBox* boxes, cons
 cudaError_t launch_amr_restrict(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
                                 int to_temp, unsigned* status, cudaStream_t s);
 cudaError_t launch_amr_timeinterp(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
+cudaError_t launch_amr_timeinterp_boxes(const AmrBlock* blocks, const AmrBox* boxes, const int2* tiles, int ntiles,
+                                        unsigned* status, cudaStream_t s);
 cudaError_t launch_amr_rotate(int* lvl, cudaStream_t s);
 cudaError_t launch_amr_enforce(const AmrBlock* blocks, const int2* tiles, int ntiles, cudaStream_t s);
 template <typename T>
@@ -127,6 +129,7 @@ extern "C" void amss_engine_destroy(amss_engine* e) {
     if (L.dtiles) cudaFree(L.dtiles);
     if (L.dtable) cudaFree(L.dtable);
     if (L.dti_tiles) cudaFree(L.dti_tiles);
+    L.dti_boxes.release();
     if (L.ditems) cudaFree(L.ditems);
     if (L.dtiles_f) cudaFree(L.dtiles_f);
     if (L.ditems_f) cudaFree(L.ditems_f);
@@ -587,6 +590,8 @@ extern "C" int amss_engine_commit(amss_engine* e) {
       AMSS_CK(cudaMalloc(&L.dti_tiles, ti.size() * sizeof(int2)));
       AMSS_CK(cudaMemcpy(L.dti_tiles, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
     }
+    if (e->levels.count(kv.first + 1))
+      if (int rc = upload_boxes(timeinterp_boxes(e, L, e->levels.at(kv.first + 1)), L.dti_boxes)) return rc;
   }
   if (e->prm.kernel == 0) {
     long long mx = 0;
@@ -853,8 +858,10 @@ static int step_level_impl(amss_engine* e, int level, double dt, bool fin = fals
 static int restrict_prolong(amss_engine* e, int l, bool same_time) {
   ELevel& F = e->levels[l];
   ELevel& C = e->levels[l - 1];
-  if (!same_time) {
-    AMSS_CK(launch_amr_timeinterp(e->dblocks, C.dti_tiles, C.nti, e->stream));
+  if (!same_time && C.dti_boxes.ntiles) {
+    // only where the prolongation below reads it
+    AMSS_CK(launch_amr_timeinterp_boxes(e->dblocks, C.dti_boxes.boxes, C.dti_boxes.tiles, C.dti_boxes.ntiles,
+                                        e->dstatus, e->stream));
     e->launches++;
   }
   const int to_temp = same_time ? 0 : 1;

@@ -116,6 +116,7 @@ struct ELevel {
   int xsync = -1, xrestrict = -1, xprolong = -1;   // transfers (index into amss_engine::xfers)
   int2* dti_tiles = nullptr;    // time-interpolation tiles (global block ids)
   int nti = 0;
+  DevBoxes dti_boxes;           // the cells the next finer level's prolongation reads (timeinterp_boxes)
   int2* dfaces = nullptr;       // outer-face points (table index, point) for k_face
   int nfaces = 0;
   DerivItem* ditems = nullptr;  // stencil-pass work items (split form)
@@ -207,6 +208,8 @@ int upload_boxes(const std::vector<AmrBox>& boxes, DevBoxes& D, int nf = 0, bool
 // Sets each level's final_pad where the final-substep regions are safe, and
 // own_ok where the same-level sync covers every ghost cell.
 void plan_final_regions(amss_engine* e);
+// Cells of C's blocks whose time interpolation F's prolongation reads.
+std::vector<AmrBox> timeinterp_boxes(amss_engine* e, const ELevel& C, const ELevel& F);
 // The final-substep region of a block (global level indices; empty: none).
 Box final_region(const amss_engine* e, const ELevel& L, const EBlock& b);
 void push_box(std::vector<AmrBox>& v, int dst, int src, const Box& b);

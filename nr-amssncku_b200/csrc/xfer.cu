@@ -295,6 +295,42 @@ void plan_final_regions(amss_engine* e) {
   }
 }
 
+// The cells of each of this rank's blocks of C (level l-1) whose time
+// interpolation the prolongation into F (level l) reads: per block the
+// bounding box of its owned cells inside the prolongation's coarse read boxes
+// (prolong3: coarse (g >> 1) - 3 .. + 2 of an even fine cell g, (g >> 1) - 2
+// .. + 3 of an odd one).  A read box's ghost cells are owned by another block
+// of C, whose own box covers them and whose values the temp sync copies.
+std::vector<AmrBox> timeinterp_boxes(amss_engine* e, const ELevel& C, const ELevel& F) {
+  std::vector<Box> reads;
+  for (const AmrBox& b : prolong_boxes(e, F, C)) {
+    Box R;
+    for (int d = 0; d < 3; ++d) {
+      const int g0 = b.lo[d], g1 = b.lo[d] + b.n[d] - 1;
+      R.lo[d] = (g0 & 1) ? (g0 >> 1) - 2 : (g0 >> 1) - 3;
+      R.hi[d] = ((g1 & 1) ? (g1 >> 1) - 2 : (g1 >> 1) - 3) + 6;
+    }
+    reads.push_back(R);
+  }
+  std::vector<AmrBox> v;
+  for (int x : C.own) {
+    const EBlock& X = e->blocks[x];
+    Box h{{0, 0, 0}, {0, 0, 0}};
+    bool any = false;
+    for (const Box& R : reads) {
+      const Box s = intersect(R, X.own);
+      if (s.empty()) continue;
+      for (int d = 0; d < 3; ++d) {
+        h.lo[d] = any ? std::min(h.lo[d], s.lo[d]) : s.lo[d];
+        h.hi[d] = any ? std::max(h.hi[d], s.hi[d]) : s.hi[d];
+      }
+      any = true;
+    }
+    if (any) push_box(v, x, x, h);
+  }
+  return v;
+}
+
 int build_xfers(amss_engine* e) {
   e->xfers.clear();
   e->staging.clear();
